@@ -1,0 +1,301 @@
+// C ABI: LU drivers and the row-interchange launchers.
+#include <algorithm>
+#include <mutex>
+
+#include "internal.h"
+#include "getrf/blocked_getrf.h"
+#include "getrf/blocked_getrf_npvt.h"
+#include "getrf/double_blocked_getrf.h"
+#include "getrf/double_blocked_getrf_npvt.h"
+#include "getrf/getrf_pivot_kernels.h"
+
+namespace hdbf {
+namespace {
+
+inline float* at(float* A, long long lda, int r, int c) { return A + (long long)c * lda + r; }
+
+hdbf_status record(hdbf_context* ctx, hdbf_status st)
+{
+    if (ctx) ctx->last_status = st;
+    return st;
+}
+
+bool bad_matrix(const void* A, int lda, int rows)
+{
+    return rows < 0 || (rows > 0 && (!A || lda < std::max(1, rows)));
+}
+
+__global__ void offset_pivots_kernel(int* p, int k, int delta)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) p[i] += delta;
+}
+
+// Compose the swaps ipiv[0..k) (1-based, minus `minus` gives rows local to
+// A(row0:n, :)) and apply them to columns [c0, c0+nc) of rows row0..n.
+hdbf_status permute_cols(hdbf_context* ctx, const GetrfWs& ws, float* A, long long lda, int n,
+                         int row0, const int* ipiv, int k, int minus, int* info,
+                         const int* col_begin, const int* col_count, int ranges)
+{
+    const int m = n - row0;
+    if (k <= 0 || m <= 0) return HDBF_STATUS_SUCCESS;
+    bool any = false;
+    for (int r = 0; r < ranges; ++r) any = any || col_count[r] > 0;
+    if (!any) return HDBF_STATUS_SUCCESS;
+    HDBF_TRY(compose_swaps(ctx, ipiv, k, minus, m, ws.src, ws.tgt, ws.count, ws.gperm, info));
+    const int max_moves = std::min(m, 2 * k);
+    for (int r = 0; r < ranges; ++r)
+        if (col_count[r] > 0)
+            HDBF_TRY(apply_moves(ctx, at(A, lda, row0, col_begin[r]), lda, col_count[r], ws.src,
+                                 ws.tgt, ws.count, max_moves, ws.temp, ws.temp_cols));
+    return HDBF_STATUS_SUCCESS;
+}
+
+// L11^{-1} applied to B (rows x cols), direct or in trsm_block row blocks
+// (src/getrf/getrf_pivot_internal.h:64-110).
+hdbf_status trsm_llu_mode(hdbf_context* ctx, int rows, int cols, float* L, long long ldl,
+                          float* B, long long ldb, bool iterative, int block)
+{
+    if (!iterative || block <= 0 || rows <= block) return trsm_llu(ctx, rows, cols, L, ldl, B, ldb);
+    for (int r = 0; r < rows; r += block) {
+        const int dr = std::min(block, rows - r);
+        HDBF_TRY(trsm_llu(ctx, dr, cols, at(L, ldl, r, r), ldl, B + r, ldb));
+        const int tr = rows - r - dr;
+        if (tr > 0)
+            HDBF_TRY(sgemm_sub(ctx, true, false, tr, cols, dr, at(L, ldl, r + dr, r), ldl, B + r,
+                               ldb, B + r + dr, ldb));
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
+// C -= L * U in row chunks (inner GEMM M-tiling,
+// src/getrf/getrf_batched_pivot_internal.h:285-323).
+hdbf_status gemm_nn_rows(hdbf_context* ctx, int rows, int cols, int k, const float* L,
+                         long long ldl, const float* U, long long ldu, float* C, long long ldc,
+                         int m_tile)
+{
+    const int tile = m_tile > 0 ? m_tile : std::max(rows, 1);
+    for (int r = 0; r < rows; r += tile)
+        HDBF_TRY(sgemm_sub(ctx, true, false, std::min(tile, rows - r), cols, k, L + r, ldl, U,
+                           ldu, C + r, ldc));
+    return HDBF_STATUS_SUCCESS;
+}
+
+enum class PivotMode { Immediate, Batched, None };
+
+// Double-blocked left-looking LU (src/getrf/double_blocked_getrf.cpp:125-191,
+// src/getrf/getrf_batched_pivot_internal.h:445-624,
+// src/getrf/double_blocked_getrf_npvt.cpp:93-144).
+hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer_nb,
+                          int inner_nb, bool iterative_outer, int trsm_block,
+                          int inner_gemm_m_tile, int* ipiv, int* info, PivotMode mode,
+                          const getrf_batched_pivot_workspace* user_ws)
+{
+    if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
+    if (mode != PivotMode::None && n > 0 && !ipiv) return HDBF_STATUS_INVALID_VALUE;
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+    if (n == 0) return last_cuda(ctx);
+    GetrfWs ws;
+    HDBF_TRY(getrf_workspace(ctx, n, &ws));
+    if (mode == PivotMode::Batched && user_ws) {
+        ws.src = user_ws->device_sources;
+        ws.tgt = user_ws->device_targets;
+        ws.temp = static_cast<float*>(user_ws->device_swap_buffer);
+        ws.temp_cols = user_ws->column_tile;
+    }
+    if (outer_nb <= 0) outer_nb = n;
+    if (inner_nb <= 0) inner_nb = outer_nb;
+    inner_nb = std::min(inner_nb, outer_nb);
+    const bool piv = mode != PivotMode::None;
+
+    for (int outer = 0; outer < n; outer += outer_nb) {
+        const int oend = outer + std::min(outer_nb, n - outer);
+        for (int inner = outer; inner < oend; inner += inner_nb) {
+            const int isz = std::min(inner_nb, oend - inner);
+            const int next = inner + isz;
+            HDBF_TRY(getrf_panel(ctx, n - inner, isz, at(A, lda, inner, inner), lda,
+                                 piv ? ipiv + inner : nullptr, inner, info, inner, piv, ws));
+            if (mode == PivotMode::Immediate) {
+                const int cb[2] = {0, next};
+                const int cc[2] = {inner, n - next};
+                HDBF_TRY(permute_cols(ctx, ws, A, lda, n, inner, ipiv + inner, isz, inner, info,
+                                      cb, cc, 2));
+            } else if (mode == PivotMode::Batched) {
+                const int cb[2] = {outer, next};
+                const int cc[2] = {inner - outer, oend - next};
+                HDBF_TRY(permute_cols(ctx, ws, A, lda, n, inner, ipiv + inner, isz, inner, info,
+                                      cb, cc, 2));
+            }
+            if (next < oend) {  // prepare_next_inner_panel
+                const int nsz = std::min(inner_nb, oend - next);
+                const int hist = next - outer;
+                HDBF_TRY(trsm_llu(ctx, hist, nsz, at(A, lda, outer, outer), lda,
+                                  at(A, lda, outer, next), lda));
+                HDBF_TRY(gemm_nn_rows(ctx, n - next, nsz, hist, at(A, lda, next, outer), lda,
+                                      at(A, lda, outer, next), lda, at(A, lda, next, next), lda,
+                                      mode == PivotMode::Batched ? inner_gemm_m_tile : 0));
+            }
+        }
+        if (mode == PivotMode::Batched) {  // outer pivot batch (:556-609)
+            if (outer > 0) {
+                const int cb[1] = {0};
+                const int cc[1] = {outer};
+                HDBF_TRY(permute_cols(ctx, ws, A, lda, n, outer, ipiv + outer, oend - outer, outer,
+                                      info, cb, cc, 1));
+            }
+            if (oend < n) {
+                const int cb[1] = {oend};
+                const int cc[1] = {std::min(outer_nb, n - oend)};
+                HDBF_TRY(permute_cols(ctx, ws, A, lda, n, 0, ipiv, oend, 0, info, cb, cc, 1));
+            }
+        }
+        if (oend < n) {  // prepare_next_outer_panel
+            const int next = oend;
+            const int nsz = std::min(outer_nb, n - next);
+            HDBF_TRY(trsm_llu_mode(ctx, next, nsz, A, lda, at(A, lda, 0, next), lda,
+                                   iterative_outer, trsm_block));
+            HDBF_TRY(sgemm_sub(ctx, true, false, n - next, nsz, next, at(A, lda, next, 0), lda,
+                               at(A, lda, 0, next), lda, at(A, lda, next, next), lda));
+        }
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
+// Blocked right-looking LU (src/getrf/blocked_getrf.cpp:15-71).
+hdbf_status getrf_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, int* ipiv,
+                          int* info, bool piv)
+{
+    if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
+    if (piv && n > 0 && !ipiv) return HDBF_STATUS_INVALID_VALUE;
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+    if (n == 0) return last_cuda(ctx);
+    GetrfWs ws;
+    HDBF_TRY(getrf_workspace(ctx, n, &ws));
+    if (nb <= 0) nb = n;
+    for (int p = 0; p < n; p += nb) {
+        const int psz = std::min(nb, n - p);
+        const int next = p + psz;
+        const int tr = n - next;
+        HDBF_TRY(getrf_panel(ctx, n - p, psz, at(A, lda, p, p), lda, piv ? ipiv + p : nullptr, p,
+                             info, p, piv, ws));
+        if (piv) {
+            const int cb[2] = {0, next};
+            const int cc[2] = {p, tr};
+            HDBF_TRY(permute_cols(ctx, ws, A, lda, n, p, ipiv + p, psz, p, info, cb, cc, 2));
+        }
+        if (tr > 0) {
+            HDBF_TRY(trsm_llu(ctx, psz, tr, at(A, lda, p, p), lda, at(A, lda, p, next), lda));
+            HDBF_TRY(sgemm_sub(ctx, true, false, tr, tr, psz, at(A, lda, next, p), lda,
+                               at(A, lda, p, next), lda, at(A, lda, next, next), lda));
+        }
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
+bool batched_ws_valid(const getrf_batched_pivot_workspace* w, int n)
+{
+    // src/getrf/getrf_batched_pivot_internal.h:43-57
+    return w && w->device_sources && w->device_targets && w->device_swap_buffer &&
+           w->host_pivots && w->host_permutation && w->host_sources && w->host_targets &&
+           w->capacity >= n && w->column_tile > 0;
+}
+
+// Context used by the handle-less kernel launchers.
+hdbf_context* launcher_context(cudaStream_t stream)
+{
+    static std::mutex mu;
+    static hdbf_context* ctx = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ctx) {
+        if (hdbf_create(&ctx) != HDBF_STATUS_SUCCESS) return nullptr;
+    }
+    ctx->stream = stream;
+    return ctx;
+}
+
+}  // namespace
+}  // namespace hdbf
+
+using namespace hdbf;
+
+extern "C" {
+
+void double_blocked_getrf(hdbf_handle h, float* A, int lda, int n, int outer_nb, int inner_nb,
+                          getrf_outer_trsm_mode outer_trsm_mode, int trsm_block, int* ipiv,
+                          int* info)
+{
+    if (!h) return;
+    record(h, getrf_db_impl(h, A, lda, n, outer_nb, inner_nb,
+                            outer_trsm_mode == getrf_outer_trsm_iterative, trsm_block, 0, ipiv,
+                            info, PivotMode::Immediate, nullptr));
+}
+
+void double_blocked_getrf_batched_pivot(hdbf_handle h, float* A, int lda, int n, int outer_nb,
+                                        int inner_nb, getrf_outer_trsm_mode outer_trsm_mode,
+                                        int trsm_block, int inner_gemm_m_tile, int* ipiv,
+                                        int* info, getrf_batched_pivot_workspace* workspace)
+{
+    if (!h) return;
+    if (!batched_ws_valid(workspace, n)) {
+        // double_blocked_getrf.cpp:263-267: info = -1 via a 0xff memset
+        if (info) cudaMemsetAsync(info, 0xff, sizeof(int), h->stream);
+        record(h, HDBF_STATUS_INVALID_VALUE);
+        return;
+    }
+    record(h, getrf_db_impl(h, A, lda, n, outer_nb, inner_nb,
+                            outer_trsm_mode == getrf_outer_trsm_iterative, trsm_block,
+                            inner_gemm_m_tile, ipiv, info, PivotMode::Batched, workspace));
+}
+
+void double_blocked_getrf_npvt(hdbf_handle h, float* A, int lda, int n, int nb, int b, int* info)
+{
+    if (!h) return;
+    record(h, getrf_db_impl(h, A, lda, n, nb, b, false, 0, 0, nullptr, info, PivotMode::None,
+                            nullptr));
+}
+
+void blocked_right_looking_getrf(hdbf_handle h, float* A, int lda, int n, int nb, int* ipiv,
+                                 int* info)
+{
+    if (!h) return;
+    record(h, getrf_rl_impl(h, A, lda, n, nb, ipiv, info, true));
+}
+
+void blocked_right_looking_getrf_npvt(hdbf_handle h, float* A, int lda, int n, int nb, int* info)
+{
+    if (!h) return;
+    record(h, getrf_rl_impl(h, A, lda, n, nb, nullptr, info, false));
+}
+
+void launch_apply_getrf_panel_pivots(float* A, int lda, int n, int panel, int panel_size,
+                                     int* pivots, cudaStream_t stream)
+{
+    if (!A || !pivots || panel_size <= 0 || n <= 0) return;
+    hdbf_context* ctx = launcher_context(stream);
+    if (!ctx) return;
+    GetrfWs ws;
+    if (getrf_workspace(ctx, n, &ws) != HDBF_STATUS_SUCCESS) return;
+    const int next = panel + panel_size;
+    const int cb[2] = {0, next};
+    const int cc[2] = {panel, n - next};
+    if (permute_cols(ctx, ws, A, lda, n, panel, pivots, panel_size, 0, nullptr, cb, cc, 2) !=
+        HDBF_STATUS_SUCCESS)
+        return;
+    offset_pivots_kernel<<<(panel_size + 255) / 256, 256, 0, stream>>>(pivots, panel_size, panel);
+}
+
+void launch_apply_getrf_permutation(float* A, int lda, int column_count, const int* sources,
+                                    const int* targets, int move_count, float* temporary,
+                                    int column_tile, cudaStream_t stream)
+{
+    if (!A || column_count <= 0 || move_count <= 0 || column_tile <= 0) return;
+    hdbf_context* ctx = launcher_context(stream);
+    if (!ctx) return;
+    // The move count is a host value here; stage it into the device word.
+    int* cnt = ctx->dev_small + kSmallMoveCount + 1;
+    cudaMemcpyAsync(cnt, &move_count, sizeof(int), cudaMemcpyHostToDevice, stream);
+    apply_moves(ctx, A, lda, column_count, sources, targets, cnt, move_count, temporary,
+                column_tile);
+}
+
+}  // extern "C"

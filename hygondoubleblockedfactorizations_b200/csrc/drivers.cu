@@ -1,0 +1,123 @@
+// Host-side building blocks: recursive diagonal Cholesky, recursive TRSMs,
+// SYRK, recursive GETRF panel.  Everything is enqueued on ctx->stream; no
+// host synchronisation.
+#include <algorithm>
+
+#include "internal.h"
+
+namespace hdbf {
+
+namespace {
+constexpr int kDiagLeaf = 64;   // potf2_small / trsm_*_small leaf order
+constexpr int kPanelLeaf = 32;  // getf2_coop width
+
+// Split point for a recursion on `n` columns with `leaf`-aligned halves.
+inline int split_at(int n, int leaf)
+{
+    int h = (n / 2 + leaf - 1) / leaf * leaf;
+    if (h <= 0 || h >= n) h = std::max(1, n - leaf);
+    return h;
+}
+}  // namespace
+
+hdbf_status potrf_diag(hdbf_context* ctx, int n, float* A, long long lda, int* info,
+                       int info_base)
+{
+    if (n <= 0) return HDBF_STATUS_SUCCESS;
+    if (n <= kDiagLeaf) return potf2_small(ctx, n, A, lda, info, info_base);
+    const int n1 = split_at(n, kDiagLeaf);
+    const int n2 = n - n1;
+    float* A21 = A + n1;
+    float* A22 = A + (long long)n1 * lda + n1;
+    HDBF_TRY(potrf_diag(ctx, n1, A, lda, info, info_base));
+    HDBF_TRY(trsm_rlt(ctx, n2, n1, A, lda, A21, lda));
+    HDBF_TRY(syrk_lower(ctx, n2, n1, A21, lda, A22, lda));
+    return potrf_diag(ctx, n2, A22, lda, info, info_base + n1);
+}
+
+hdbf_status trsm_rlt(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
+                     float* B, long long ldb)
+{
+    if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
+    if (cols <= kDiagLeaf) return trsm_rlt_small(ctx, rows, cols, L, ldl, B, ldb);
+    const int c1 = split_at(cols, kDiagLeaf);
+    const int c2 = cols - c1;
+    HDBF_TRY(trsm_rlt(ctx, rows, c1, L, ldl, B, ldb));
+    // B2 -= X1 * L21^T, L21 = L(c1:cols, 0:c1)
+    HDBF_TRY(sgemm_sub(ctx, false, false, rows, c2, c1, B, ldb, L + c1, ldl,
+                       B + (long long)c1 * ldb, ldb));
+    return trsm_rlt(ctx, rows, c2, L + (long long)c1 * ldl + c1, ldl, B + (long long)c1 * ldb,
+                    ldb);
+}
+
+hdbf_status trsm_llu(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
+                     float* B, long long ldb)
+{
+    if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
+    if (rows <= kDiagLeaf) return trsm_llu_small(ctx, rows, cols, L, ldl, B, ldb);
+    const int r1 = split_at(rows, kDiagLeaf);
+    const int r2 = rows - r1;
+    HDBF_TRY(trsm_llu(ctx, r1, cols, L, ldl, B, ldb));
+    // B2 -= L21 * X1
+    HDBF_TRY(sgemm_sub(ctx, true, false, r2, cols, r1, L + r1, ldl, B, ldb, B + r1, ldb));
+    return trsm_llu(ctx, r2, cols, L + (long long)r1 * ldl + r1, ldl, B + r1, ldb);
+}
+
+hdbf_status syrk_lower(hdbf_context* ctx, int n, int k, const float* A, long long lda,
+                       float* C, long long ldc)
+{
+    return sgemm_sub(ctx, false, true, n, n, k, A, lda, A, lda, C, ldc);
+}
+
+hdbf_status getrf_workspace(hdbf_context* ctx, int n, GetrfWs* ws)
+{
+    hdbf_status st;
+    const size_t need = hdbf_workspace_bytes_for(n);
+    char* base = static_cast<char*>(workspace(ctx, need, &st));
+    if (!base) return st;
+    size_t off = getf2_coop_scratch_bytes();  // the coop scratch sits at offset 0
+    const size_t ints = align_up(size_t(std::max(n, 1)) * sizeof(int), 256);
+    ws->src = reinterpret_cast<int*>(base + off);
+    off += ints;
+    ws->tgt = reinterpret_cast<int*>(base + off);
+    off += ints;
+    ws->gperm = reinterpret_cast<int*>(base + off);
+    off += ints;
+    ws->temp = reinterpret_cast<float*>(base + off);
+    ws->temp_cols = 64;
+    ws->count = ctx->dev_small + kSmallMoveCount;
+    return HDBF_STATUS_SUCCESS;
+}
+
+// Recursive (Toledo/Gustavson) LU of an m x w panel; leaves of kPanelLeaf
+// columns go to the cooperative kernel.  ipiv receives (local row + 1 +
+// ipiv_add) for the panel's w columns.
+hdbf_status getrf_panel(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
+                        int ipiv_add, int* info, int info_base, bool pivot, const GetrfWs& ws)
+{
+    if (m <= 0 || w <= 0) return HDBF_STATUS_SUCCESS;
+    if (w <= kPanelLeaf) return getf2_coop(ctx, m, w, A, lda, ipiv, ipiv_add, info, info_base, pivot);
+    const int w1 = split_at(w, kPanelLeaf);
+    const int w2 = w - w1;
+    HDBF_TRY(getrf_panel(ctx, m, w1, A, lda, ipiv, ipiv_add, info, info_base, pivot, ws));
+    float* A12 = A + (long long)w1 * lda;
+    if (pivot) {
+        HDBF_TRY(compose_swaps(ctx, ipiv, w1, ipiv_add, m, ws.src, ws.tgt, ws.count, ws.gperm,
+                               info));
+        HDBF_TRY(apply_moves(ctx, A12, lda, w2, ws.src, ws.tgt, ws.count,
+                             std::min(m, 2 * w1), ws.temp, ws.temp_cols));
+    }
+    HDBF_TRY(trsm_llu(ctx, w1, w2, A, lda, A12, lda));
+    HDBF_TRY(sgemm_sub(ctx, true, false, m - w1, w2, w1, A + w1, lda, A12, lda, A12 + w1, lda));
+    HDBF_TRY(getrf_panel(ctx, m - w1, w2, A12 + w1, lda, pivot ? ipiv + w1 : nullptr,
+                         ipiv_add + w1, info, info_base + w1, pivot, ws));
+    if (pivot) {
+        HDBF_TRY(compose_swaps(ctx, ipiv + w1, w2, ipiv_add + w1, m - w1, ws.src, ws.tgt,
+                               ws.count, ws.gperm, info));
+        HDBF_TRY(apply_moves(ctx, A + w1, lda, w1, ws.src, ws.tgt, ws.count,
+                             std::min(m - w1, 2 * w2), ws.temp, ws.temp_cols));
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
+}  // namespace hdbf

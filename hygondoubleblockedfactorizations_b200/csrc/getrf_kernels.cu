@@ -1,0 +1,460 @@
+// GETRF panel, pivot composition and row-permutation kernels (FP32).
+//
+// getf2_coop replaces rocsolver_sgetrf's unblocked leaf on the tall panel
+// (src/getrf/getrf_pivot_internal.h:17-39): one cooperative launch factors an
+// m x w (w <= 32) column block with partial pivoting.  Each CTA keeps a
+// contiguous slice of rows of the block resident in shared memory; per column
+// the CTAs publish their local |max| candidate (value, row and the full
+// candidate row) and the owner of the diagonal row publishes that row, then
+// meet at one bounded grid barrier, after which every CTA picks the same
+// global winner (largest |a|, lowest row on ties -- LAPACK ISAMAX), swaps,
+// scales by the reciprocal pivot (division when |pivot| < FLT_MIN, as
+// xGETF2) and applies the rank-1 update to its own rows.
+//
+// compose_swaps + apply_moves replace apply_panel_pivots_kernel
+// (src/getrf/getrf_pivot_kernels.hip:14-45) and the host-side permutation
+// batching (src/getrf/getrf_batched_pivot_internal.h:59-223): a LAPACK swap
+// sequence is composed on the GPU into a list of (source, target) row moves,
+// then applied to column tiles with a gather into shared memory followed by a
+// scatter -- no host round trip.
+#include <cfloat>
+#include <climits>
+
+#include "internal.h"
+
+namespace hdbf {
+namespace {
+
+constexpr int kCoopThreads = 256;
+constexpr int kCoopMaxW = 32;
+constexpr int kCoopMaxGrid = 1024;
+constexpr int kCandStride = kCoopMaxW + 2;  // |val|, row, w row values
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded sense-reversing grid barrier.  Returns false (and records a timeout
+// in *err) if the other CTAs did not arrive within the poll limit.
+__device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err,
+                             int* s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned g = ld_acquire_u32(gen);
+        __threadfence();
+        const unsigned arrived = atomicAdd(count, 1u) + 1u;
+        if (arrived == nblocks) {
+            atomicExch(count, 0u);
+            __threadfence();
+            st_release_u32(gen, g + 1u);
+        } else {
+            unsigned polls = 0;
+            while (ld_acquire_u32(gen) == g) {
+                if (++polls > kSpinLimit) {
+                    ok = 0;
+                    atomicExch(err, kErrTimeout);
+                    break;
+                }
+                if (polls > 64) __nanosleep(64);
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// Candidate (v, i) beats (bv, bi): a real row beats none, then larger |a|,
+// then the lower row (LAPACK ISAMAX returns the first maximum).
+__device__ __forceinline__ bool better(float v, int i, float bv, int bi)
+{
+    if (i == INT_MAX) return false;
+    if (bi == INT_MAX) return true;
+    return v > bv || (v == bv && i < bi);
+}
+
+__global__ void __launch_bounds__(kCoopThreads)
+getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int ipiv_add,
+                  int* info, int info_base, float* scr, unsigned* bar_count, unsigned* bar_gen,
+                  int* err, int pivot)
+{
+    extern __shared__ float tile[];  // tile[c * rpc + r]
+    __shared__ float prow[kCoopMaxW];
+    __shared__ float orow[kCoopMaxW];
+    __shared__ float red_v[kCoopThreads / 32];
+    __shared__ int red_i[kCoopThreads / 32];
+    __shared__ int s_best_row, s_win_cta, s_ok;
+
+    const int G = gridDim.x;
+    const int cta = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int r0 = cta * rpc;
+    const int nr = max(0, min(m, r0 + rpc) - r0);
+
+    for (int c = 0; c < w; ++c)
+        for (int r = tid; r < nr; r += kCoopThreads)
+            tile[c * rpc + r] = A[(long long)c * lda + (r0 + r)];
+    __syncthreads();
+
+    float* cand_base = scr;                                   // [2][G][kCandStride]
+    float* diag_base = scr + 2 * kCoopMaxGrid * kCandStride;  // [2][kCoopMaxW]
+    const int steps = min(m, w);
+    bool alive = true;
+
+    for (int j = 0; j < steps && alive; ++j) {
+        // Local candidate: largest |a(r, j)| over owned rows r >= j, lowest row on ties.
+        float bv = -1.f;
+        int bi = INT_MAX;
+        for (int r = tid; pivot && r < nr; r += kCoopThreads) {
+            const int gr = r0 + r;
+            if (gr >= j) {
+                const float v = fabsf(tile[j * rpc + r]);
+                if (bi == INT_MAX || v > bv) { bv = v; bi = gr; }
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ov = __shfl_down_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 1; q < kCoopThreads / 32; ++q)
+                if (better(red_v[q], red_i[q], bv, bi)) { bv = red_v[q]; bi = red_i[q]; }
+            s_best_row = bi;
+        }
+        __syncthreads();
+        const int par = j & 1;
+        float* cand = cand_base + ((long long)par * kCoopMaxGrid + cta) * kCandStride;
+        const int my_best = s_best_row;
+        if (tid == 0) {
+            cand[0] = bv;
+            cand[1] = __int_as_float(my_best);
+        }
+        if (tid < w && my_best != INT_MAX) cand[2 + tid] = tile[tid * rpc + (my_best - r0)];
+        float* drow = diag_base + par * kCoopMaxW;
+        if (j >= r0 && j < r0 + nr && tid < w) drow[tid] = tile[tid * rpc + (j - r0)];
+
+        if (!grid_barrier(bar_count, bar_gen, (unsigned)G, err, &s_ok)) { alive = false; break; }
+
+        // Global winner (identical on every CTA); without pivoting the
+        // diagonal row is the pivot row.
+        if (!pivot) {
+            if (tid == 0) { s_best_row = j; s_win_cta = -1; }
+        } else if (warp == 0) {
+            float gv = -1.f;
+            int gi = INT_MAX, gc = 0;
+            for (int q = lane; q < G; q += 32) {
+                const float* cq = cand_base + ((long long)par * kCoopMaxGrid + q) * kCandStride;
+                const float v = __ldcg(cq);
+                const int i = __float_as_int(__ldcg(cq + 1));
+                if (better(v, i, gv, gi)) { gv = v; gi = i; gc = q; }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ov = __shfl_down_sync(0xffffffffu, gv, off);
+                const int oi = __shfl_down_sync(0xffffffffu, gi, off);
+                const int oc = __shfl_down_sync(0xffffffffu, gc, off);
+                if (better(ov, oi, gv, gi)) { gv = ov; gi = oi; gc = oc; }
+            }
+            if (lane == 0) { s_best_row = gi; s_win_cta = gc; }
+        }
+        __syncthreads();
+        const int p = s_best_row;
+        if (tid < w) {
+            orow[tid] = __ldcg(drow + tid);
+            if (s_win_cta >= 0) {
+                const float* cw =
+                    cand_base + ((long long)par * kCoopMaxGrid + s_win_cta) * kCandStride;
+                prow[tid] = __ldcg(cw + 2 + tid);
+            } else {
+                prow[tid] = orow[tid];
+            }
+        }
+        if (pivot && cta == 0 && tid == 0) ipiv[j] = p + 1 + ipiv_add;
+        __syncthreads();
+        if (p != j && tid < w) {
+            if (j >= r0 && j < r0 + nr) tile[tid * rpc + (j - r0)] = prow[tid];
+            if (p >= r0 && p < r0 + nr) tile[tid * rpc + (p - r0)] = orow[tid];
+        }
+        __syncthreads();
+        const float piv = prow[j];
+        if (piv != 0.f) {
+            const bool recip = fabsf(piv) >= FLT_MIN;
+            const float rcp = 1.0f / piv;
+            for (int r = tid; r < nr; r += kCoopThreads) {
+                if (r0 + r > j) {
+                    float l = tile[j * rpc + r];
+                    l = recip ? l * rcp : l / piv;
+                    tile[j * rpc + r] = l;
+                    for (int c = j + 1; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
+                }
+            }
+        } else {
+            if (cta == 0 && tid == 0 && info) atomicCAS(info, 0, info_base + j + 1);
+            for (int r = tid; r < nr; r += kCoopThreads) {
+                if (r0 + r > j) {
+                    const float l = tile[j * rpc + r];
+                    for (int c = j + 1; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    for (int c = 0; c < w; ++c)
+        for (int r = tid; r < nr; r += kCoopThreads)
+            A[(long long)c * lda + (r0 + r)] = tile[c * rpc + r];
+}
+
+// ------------------------------------------------------------ compose swaps
+constexpr int kComposeThreads = 1024;
+
+__global__ void __launch_bounds__(kComposeThreads)
+compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m, int* src,
+                     int* tgt, int* count, int* gperm, int use_smem, int* info, int* err)
+{
+    extern __shared__ int sperm[];
+    __shared__ int warp_tot[kComposeThreads / 32];
+    __shared__ int s_base, s_bad, s_chunk;
+    int* perm = use_smem ? sperm : gperm;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < m; q += kComposeThreads) perm[q] = q;
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    if (tid == 0) {
+        int bad = 0;
+        for (int i = 0; i < k; ++i) {
+            const int b = ipiv[i] - 1 - ipiv_minus;
+            if (b < i || b >= m) { bad = 1; break; }
+            if (b != i) {
+                const int t = perm[i];
+                perm[i] = perm[b];
+                perm[b] = t;
+            }
+        }
+        s_bad = bad;
+        s_base = 0;
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (tid == 0) {
+            *count = 0;
+            if (info) atomicExch(info, -1);
+            atomicExch(err, kErrBadPivot);
+        }
+        return;
+    }
+    // Ordered compaction of the rows whose content changed.
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int q0 = 0; q0 < m; q0 += kComposeThreads) {
+        const int q = q0 + tid;
+        const int s = (q < m) ? perm[q] : q;
+        const bool moved = (q < m) && (s != q);
+        const unsigned ball = __ballot_sync(0xffffffffu, moved);
+        const int within = __popc(ball & ((1u << lane) - 1u));
+        if (lane == 0) warp_tot[warp] = __popc(ball);
+        __syncthreads();
+        if (tid == 0) {
+            int run = 0;
+            for (int wv = 0; wv < kComposeThreads / 32; ++wv) {
+                const int t = warp_tot[wv];
+                warp_tot[wv] = run;
+                run += t;
+            }
+            s_chunk = run;
+        }
+        __syncthreads();
+        if (moved) {
+            const int pos = s_base + warp_tot[warp] + within;
+            src[pos] = s;
+            tgt[pos] = q;
+        }
+        __syncthreads();
+        if (tid == 0) s_base += s_chunk;
+        __syncthreads();
+    }
+    if (tid == 0) *count = s_base;
+}
+
+// ------------------------------------------------------------ apply moves
+constexpr int kApplyThreads = 256;
+
+// Columns [blockIdx.x*cpc, +cpc): gather every source row into shared memory,
+// then scatter to the targets.  Sources and targets are the same row set, so
+// reading everything before writing anything is race-free per column.
+__global__ void __launch_bounds__(kApplyThreads)
+apply_moves_smem_kernel(float* A, long long lda, int ncols, const int* __restrict__ src,
+                        const int* __restrict__ tgt, const int* __restrict__ count, int cpc,
+                        int cap)
+{
+    extern __shared__ float buf[];
+    const int cnt = min(*count, cap);
+    if (cnt <= 0) return;
+    const int c0 = blockIdx.x * cpc;
+    const int nc = min(cpc, ncols - c0);
+    for (int cc = 0; cc < nc; ++cc) {
+        const float* col = A + (long long)(c0 + cc) * lda;
+        for (int i = threadIdx.x; i < cnt; i += kApplyThreads) buf[cc * cap + i] = col[src[i]];
+    }
+    __syncthreads();
+    for (int cc = 0; cc < nc; ++cc) {
+        float* col = A + (long long)(c0 + cc) * lda;
+        for (int i = threadIdx.x; i < cnt; i += kApplyThreads) col[tgt[i]] = buf[cc * cap + i];
+    }
+}
+
+__global__ void gather_rows_kernel(const float* A, long long lda, int ncols,
+                                   const int* __restrict__ src, const int* __restrict__ count,
+                                   int cap, float* temp)
+{
+    const int cnt = min(*count, cap);
+    const long long total = (long long)cnt * ncols;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % cnt);
+        const long long c = idx / cnt;
+        temp[c * cap + i] = A[c * lda + src[i]];
+    }
+}
+
+__global__ void scatter_rows_kernel(float* A, long long lda, int ncols,
+                                    const int* __restrict__ tgt, const int* __restrict__ count,
+                                    int cap, const float* temp)
+{
+    const int cnt = min(*count, cap);
+    const long long total = (long long)cnt * ncols;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % cnt);
+        const long long c = idx / cnt;
+        A[c * lda + tgt[i]] = temp[c * cap + i];
+    }
+}
+
+}  // namespace
+
+size_t getf2_coop_scratch_bytes()
+{
+    return align_up((size_t)(2 * kCoopMaxGrid * kCandStride + 2 * kCoopMaxW) * sizeof(float),
+                    256);
+}
+
+hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
+                       int ipiv_add, int* info, int info_base, bool pivot)
+{
+    int piv_flag = pivot ? 1 : 0;
+    if (m <= 0 || w <= 0) return HDBF_STATUS_SUCCESS;
+    if (w > kCoopMaxW) return HDBF_STATUS_INVALID_VALUE;
+    hdbf_status st;
+    float* scr = static_cast<float*>(workspace(ctx, getf2_coop_scratch_bytes(), &st));
+    if (!scr) return st;
+
+    // Grid: about 256 rows per CTA, at most one CTA per SM (co-residency is
+    // guaranteed by the cooperative launch), shared slice <= max opt-in.
+    static int occ_cached = -1;
+    const size_t smem_cap = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
+    int G = (m + 255) / 256;
+    if (G > ctx->sm_count) G = ctx->sm_count;
+    if (G > kCoopMaxGrid) G = kCoopMaxGrid;
+    if (G < 1) G = 1;
+    int rpc = (m + G - 1) / G;
+    size_t smem = (size_t)rpc * w * sizeof(float);
+    if (smem > smem_cap) return HDBF_STATUS_NOT_SUPPORTED;
+    if (occ_cached < 0) {
+        cudaFuncSetAttribute(getf2_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_cap);
+        occ_cached = 1;
+    }
+    unsigned* bar_count = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallBarCount);
+    unsigned* bar_gen = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallBarGen);
+    int* err = ctx->dev_small + kSmallErr;
+    ProfScope prof(ctx, kClsPanel, (double)m * w * w - (double)w * w * w / 3.0, 8.0 * m * w);
+    void* args[] = {&m, &w, &A, &lda, &rpc, &ipiv, &ipiv_add, &info, &info_base,
+                    &scr, &bar_count, &bar_gen, &err, &piv_flag};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)getf2_coop_kernel, dim3(G),
+                                                dim3(kCoopThreads), args, smem, ctx->stream);
+    ctx->launches++;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
+hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_minus, int m,
+                          int* src, int* tgt, int* count, int* gperm, int* info)
+{
+    if (k <= 0 || m <= 0) return HDBF_STATUS_SUCCESS;
+    const size_t smem = (size_t)m * sizeof(int);
+    const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
+    const int use_smem = smem <= cap ? 1 : 0;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(compose_swaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)cap);
+        configured = true;
+    }
+    if (!use_smem && !gperm) return HDBF_STATUS_INVALID_VALUE;
+    ProfScope prof(ctx, kClsCompose, 0.0, 4.0 * k + 8.0 * m);
+    compose_swaps_kernel<<<1, kComposeThreads, use_smem ? smem : 0, ctx->stream>>>(
+        ipiv, k, ipiv_minus, m, src, tgt, count, gperm, use_smem, info,
+        ctx->dev_small + kSmallErr);
+    ctx->launches++;
+    return last_cuda(ctx);
+}
+
+hdbf_status apply_moves(hdbf_context* ctx, float* A, long long lda, int ncols,
+                        const int* src, const int* tgt, const int* count, int max_moves,
+                        float* temp, long long temp_cols)
+{
+    if (ncols <= 0 || max_moves <= 0) return HDBF_STATUS_SUCCESS;
+    const size_t per_col = (size_t)max_moves * sizeof(float);
+    const size_t budget = 48 * 1024;
+    static bool configured = false;
+    if (!configured) {
+        const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
+        cudaFuncSetAttribute(apply_moves_smem_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+        configured = true;
+    }
+    const size_t hard_cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
+    ProfScope prof(ctx, kClsMoves, 0.0, 8.0 * (double)max_moves * ncols);
+    if (per_col <= hard_cap) {
+        int cpc = (int)(budget / per_col);
+        if (cpc < 1) cpc = 1;
+        if (cpc > 16) cpc = 16;
+        const int grid = (ncols + cpc - 1) / cpc;
+        apply_moves_smem_kernel<<<grid, kApplyThreads, per_col * cpc, ctx->stream>>>(
+            A, lda, ncols, src, tgt, count, cpc, max_moves);
+        ctx->launches++;
+        return last_cuda(ctx);
+    }
+    if (!temp || temp_cols <= 0) return HDBF_STATUS_INVALID_VALUE;
+    for (long long c = 0; c < ncols; c += temp_cols) {
+        const int nc = (int)((ncols - c) < temp_cols ? (ncols - c) : temp_cols);
+        const long long total = (long long)nc * max_moves;
+        const int grid = (int)((total + 255) / 256 < 65535 ? (total + 255) / 256 : 65535);
+        gather_rows_kernel<<<grid, 256, 0, ctx->stream>>>(A + c * lda, lda, nc, src, count,
+                                                          max_moves, temp);
+        scatter_rows_kernel<<<grid, 256, 0, ctx->stream>>>(A + c * lda, lda, nc, tgt, count,
+                                                           max_moves, temp);
+        ctx->launches += 2;
+    }
+    return last_cuda(ctx);
+}
+
+}  // namespace hdbf

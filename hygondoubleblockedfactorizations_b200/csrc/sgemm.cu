@@ -1,0 +1,209 @@
+// FP32 SIMT trailing-update GEMM / SYRK:  C -= A * op(B).
+//
+// Replaces the reference's rocblas_sgemm (N,T) and (N,N) update calls
+// (src/gemm/update_gemm.cpp:29-44, src/getrf/getrf_npvt_internal.h:109-124)
+// and rocblas_ssyrk lower (src/syrk/kblocked_syrk.cpp:33-45).
+//
+// Design: 128x128 CTA tile, K-step 8, 256 threads each owning an 8x8
+// register micro-tile (two 4-row x two 4-column quads, so the shared-memory
+// fragment reads are float4 broadcasts), double-buffered shared memory fed
+// from a register prefetch of the next K-slab, one __syncthreads per slab.
+// Two CTAs per SM (<= 128 registers per thread).  Every product is an IEEE
+// FP32 FFMA; accumulation runs in k order from zero, then C - acc.
+#include "internal.h"
+
+namespace hdbf {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 128;
+constexpr int BK = 8;
+constexpr int NTHR = 256;
+
+template <bool VEC>
+__device__ __forceinline__ float4 load_col4(const float* p, int row, int rows_valid)
+{
+    // Four consecutive rows of one column; rows beyond rows_valid read 0.
+    float4 v;
+    if (VEC && row + 3 < rows_valid) {
+        v = __ldg(reinterpret_cast<const float4*>(p));
+    } else {
+        v.x = (row + 0 < rows_valid) ? __ldg(p + 0) : 0.f;
+        v.y = (row + 1 < rows_valid) ? __ldg(p + 1) : 0.f;
+        v.z = (row + 2 < rows_valid) ? __ldg(p + 2) : 0.f;
+        v.w = (row + 3 < rows_valid) ? __ldg(p + 3) : 0.f;
+    }
+    return v;
+}
+
+template <bool NN, bool VEC, bool TRI>
+__global__ void __launch_bounds__(NTHR, 2)
+sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda,
+                 const float* __restrict__ B, long long ldb, float* __restrict__ C,
+                 long long ldc, int tiles_m)
+{
+    const int tm = blockIdx.x % tiles_m;
+    const int tn = blockIdx.x / tiles_m;
+    const int m0 = tm * BM;
+    const int n0 = tn * BN;
+    if (TRI && m0 + BM <= n0) return;  // tile strictly above the diagonal
+
+    constexpr int BSTR = NN ? BN + 4 : BN;  // pad breaks STS bank conflicts (NN)
+    __shared__ __align__(16) float As[2][BK][BM];
+    __shared__ __align__(16) float Bs[2][BK][BSTR];
+
+    const int tid = threadIdx.x;
+    const int ak = tid >> 5;
+    const int ar = (tid & 31) * 4;
+    const int bk = NN ? (tid & 1) * 4 : (tid >> 5);
+    const int bn = NN ? (tid >> 1) : (tid & 31) * 4;
+
+    const float* a_ptr = A + (long long)ak * lda + (m0 + ar);
+    const float* b_ptr = NN ? B + (long long)(n0 + bn) * ldb + bk
+                            : B + (long long)bk * ldb + (n0 + bn);
+    const long long a_step = (long long)BK * lda;
+    const long long b_step = NN ? (long long)BK : (long long)BK * ldb;
+
+    auto fetch_a = [&](int k0) -> float4 {
+        if (k0 + ak < K) return load_col4<VEC>(a_ptr, m0 + ar, M);
+        return make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    auto fetch_b = [&](int k0) -> float4 {
+        if (NN) {
+            if (n0 + bn < N) return load_col4<VEC>(b_ptr, k0 + bk, K);
+            return make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (k0 + bk < K) return load_col4<VEC>(b_ptr, n0 + bn, N);
+        return make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    auto stash = [&](int buf, float4 ra, float4 rb) {
+        *reinterpret_cast<float4*>(&As[buf][ak][ar]) = ra;
+        if (NN) {
+            Bs[buf][bk + 0][bn] = rb.x;
+            Bs[buf][bk + 1][bn] = rb.y;
+            Bs[buf][bk + 2][bn] = rb.z;
+            Bs[buf][bk + 3][bn] = rb.w;
+        } else {
+            *reinterpret_cast<float4*>(&Bs[buf][bk][bn]) = rb;
+        }
+    };
+
+    const int tx = tid & 15;
+    const int ty = tid >> 4;
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+    float4 ra = fetch_a(0);
+    float4 rb = fetch_b(0);
+    stash(0, ra, rb);
+    __syncthreads();
+
+    const int ktiles = (K + BK - 1) / BK;
+    int buf = 0;
+    for (int kt = 0; kt < ktiles; ++kt) {
+        const bool more = kt + 1 < ktiles;
+        if (more) {
+            a_ptr += a_step;
+            b_ptr += b_step;
+            ra = fetch_a((kt + 1) * BK);
+            rb = fetch_b((kt + 1) * BK);
+        }
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][64 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        if (more) stash(buf ^ 1, ra, rb);
+        __syncthreads();
+        buf ^= 1;
+    }
+
+    // Epilogue: C -= acc.
+    const bool full_rows = (m0 + BM <= M);
+    const bool full_cols = (n0 + BN <= N);
+    const bool below_diag = !TRI || (m0 >= n0 + BN);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+        if (col >= N) continue;
+        float* cp = C + (long long)col * ldc;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int row = m0 + h * 64 + ty * 4;
+            if (VEC && full_rows && full_cols && below_diag) {
+                float4 c = *reinterpret_cast<float4*>(cp + row);
+                c.x -= acc[h * 4 + 0][j];
+                c.y -= acc[h * 4 + 1][j];
+                c.z -= acc[h * 4 + 2][j];
+                c.w -= acc[h * 4 + 3][j];
+                *reinterpret_cast<float4*>(cp + row) = c;
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = row + i;
+                    if (r < M && (!TRI || r >= col)) cp[r] -= acc[h * 4 + i][j];
+                }
+            }
+        }
+    }
+}
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <bool NN, bool VEC, bool TRI>
+void launch_sub(cudaStream_t s, int M, int N, int K, const float* A, long long lda,
+                const float* B, long long ldb, float* C, long long ldc)
+{
+    const int tiles_m = (M + BM - 1) / BM;
+    const int tiles_n = (N + BN - 1) / BN;
+    const long long grid = (long long)tiles_m * tiles_n;
+    sgemm_sub_kernel<NN, VEC, TRI><<<(unsigned)grid, NTHR, 0, s>>>(M, N, K, A, lda, B, ldb,
+                                                                  C, ldc, tiles_m);
+}
+
+}  // namespace
+
+hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
+                      const float* A, long long lda, const float* B, long long ldb,
+                      float* C, long long ldc)
+{
+    if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
+    if (!A || !B || !C) return HDBF_STATUS_INVALID_VALUE;
+    const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+    if (tiles > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
+    const bool vec = aligned16(A) && aligned16(B) && aligned16(C) && (lda % 4 == 0) &&
+                     (ldb % 4 == 0) && (ldc % 4 == 0);
+    cudaStream_t s = ctx->stream;
+    double flops = 2.0 * (double)M * N * K;
+    if (lower_only) {
+        // only entries with row >= col: sum over cols j < min(M,N) of (M - j)
+        const double d = (double)(M < N ? M : N);
+        flops = 2.0 * (double)K * (d * (double)M - d * (d - 1.0) / 2.0);
+    }
+    ProfScope prof(ctx, kClsGemm, flops, 4.0 * ((double)M * K + (double)N * K + 2.0 * M * N));
+#define HDBF_SUB(NNv, VECv, TRIv) launch_sub<NNv, VECv, TRIv>(s, M, N, K, A, lda, B, ldb, C, ldc)
+    if (nn) {
+        if (vec) { if (lower_only) HDBF_SUB(true, true, true); else HDBF_SUB(true, true, false); }
+        else { if (lower_only) HDBF_SUB(true, false, true); else HDBF_SUB(true, false, false); }
+    } else {
+        if (vec) { if (lower_only) HDBF_SUB(false, true, true); else HDBF_SUB(false, true, false); }
+        else { if (lower_only) HDBF_SUB(false, false, true); else HDBF_SUB(false, false, false); }
+    }
+#undef HDBF_SUB
+    ctx->launches++;
+    return last_cuda(ctx);
+}
+
+}  // namespace hdbf

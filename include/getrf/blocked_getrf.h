@@ -1,0 +1,18 @@
+/*
+ * Blocked right-looking LU with partial pivoting, FP32.
+ * Drop-in for reference include/getrf/blocked_getrf.h:9-15
+ * (src/getrf/blocked_getrf.cpp:15-71).
+ */
+#pragma once
+#include "hdbf/hdbf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void blocked_right_looking_getrf(hdbf_handle handle, float* A, int lda, int n, int nb,
+                                 int* ipiv, int* info);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,18 @@
+/*
+ * Double-blocked left-looking LU without pivoting, FP32.
+ * Drop-in for reference include/getrf/double_blocked_getrf_npvt.h:9-15
+ * (src/getrf/double_blocked_getrf_npvt.cpp:93-144).
+ */
+#pragma once
+#include "hdbf/hdbf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void double_blocked_getrf_npvt(hdbf_handle handle, float* A, int lda, int n, int nb,
+                               int b, int* info);
+
+#ifdef __cplusplus
+}
+#endif

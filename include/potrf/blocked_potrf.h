@@ -1,0 +1,18 @@
+/*
+ * Classic blocked right-looking Cholesky (lower), FP32.
+ * Drop-in for reference include/potrf/blocked_potrf.h:9-14
+ * (src/potrf/blocked_potrf.cpp:126-206).
+ */
+#pragma once
+#include "hdbf/hdbf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void blocked_right_looking_potrf(hdbf_handle handle, float* A, int lda, int n, int nb,
+                                 int* info);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,30 @@
+/*
+ * Recursive Cholesky (lower), FP32.
+ * Drop-in for reference include/potrf/recursive_potrf.h:10-37
+ * (src/potrf/recursive_potrf.cpp:17-174, 241-388).
+ *
+ * Splits n -> n/2 until n <= nb, then factors the leaf with this library's
+ * blocked diagonal kernel.  `pool` may be NULL; all work is stream-ordered on
+ * the handle's stream (the reference's per-level host synchronisation of pool
+ * streams, src/syrk/batched_syrk.cpp:15-22, is not needed).
+ */
+#pragma once
+#include "hdbf/hdbf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* reference recursive_potrf.h:10-15 */
+void recursive_potrf(hdbf_handle handle, StreamPool* pool, float* A, int lda, int n,
+                     int nb, int* info);
+
+/* reference recursive_potrf.h:17-22 (TRSM updates tiled at 8192,
+ * src/trsm/recursive_trsm.cpp:12, 82-122) */
+void recursive_potrf_tiled_trsm(hdbf_handle handle, StreamPool* pool, float* A, int lda,
+                                int n, int nb, int* info);
+
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,281 @@
+"""CPU oracle for the dense-factorization hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this package, and only as the checker or the timed CPU
+reference; the CUDA library never routes through it.
+
+Contents
+--------
+* ``potrf_residual`` / ``getrf_residual`` -- C restatement (``residual.c``) of
+  the reference's CPU FP64 residual, ``include/utils/benchmark/cpu_fp64_residual.h:73-201``.
+* ``potrf_residual_blas`` / ``getrf_residual_blas`` -- the same quantity with the
+  FP64 product done by host BLAS (numpy), the analogue of the reference's
+  ``HYGON_CPU_FP64_USE_CBLAS`` mode (``cpu_fp64_residual.h:52-71``); pinned
+  against the C version on small sizes by the tests.
+* ``double_blocked_potrf`` / ``double_blocked_getrf`` -- plain-C FP32 restatement
+  of the reference loops (``factor.c``).
+* ``lapack_spotrf`` / ``lapack_sgetrf`` -- host LAPACK (SciPy's OpenBLAS), the
+  pivot-sequence reference and the timed CPU baseline.
+* ``uniform_pm1`` / ``spd_gram`` / ``general_uniform`` -- the seeded input
+  generators (counter-based RNG, bit-identical to the device generator).
+* ``scaled`` -- residual / (n * eps32), eps32 = 2**-23 (FLT_EPSILON).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+EPS32 = float(np.finfo(np.float32).eps)  # 2**-23
+EPS64 = float(np.finfo(np.float64).eps)
+
+_lib = None
+
+
+def build() -> str:
+    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
+    if os.path.isdir("/root/reference/include"):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    return os.path.join(_HERE, "liboracle.so")
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        dp, ip, i = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int
+        for name in ("oracle_potrf_residual_f32", "oracle_potrf_residual_f64"):
+            f = getattr(L, name)
+            f.restype = ctypes.c_double
+            f.argtypes = [dp, dp, i, i, i, ip]
+        for name in ("oracle_getrf_residual_f32", "oracle_getrf_residual_f64"):
+            f = getattr(L, name)
+            f.restype = ctypes.c_double
+            f.argtypes = [dp, dp, dp, i, i, i, i, ip]
+        L.oracle_double_blocked_potrf.restype = i
+        L.oracle_double_blocked_potrf.argtypes = [dp, i, i, i, i, i]
+        L.oracle_double_blocked_getrf.restype = i
+        L.oracle_double_blocked_getrf.argtypes = [dp, i, i, i, i, dp]
+        L.oracle_parse_seed.restype = i
+        L.oracle_parse_seed.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint)]
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own residual header compiled in place (oracle/_ref)."""
+    path = os.path.join(_HERE, "_ref", "libref_residual.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    dp, ip, i = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int
+    for name in ("ref_potrf_residual_f32", "ref_potrf_residual_f64"):
+        f = getattr(L, name)
+        f.restype = ctypes.c_double
+        f.argtypes = [dp, dp, i, i, i, ip]
+    for name in ("ref_getrf_residual_f32", "ref_getrf_residual_f64"):
+        f = getattr(L, name)
+        f.restype = ctypes.c_double
+        f.argtypes = [dp, dp, dp, i, i, i, i, ip]
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _colmajor(a, dtype):
+    """Return (flat column-major buffer, lda) for a 2-D array or (flat, lda) tuple."""
+    if isinstance(a, tuple):
+        flat, lda = a
+        return np.ascontiguousarray(flat, dtype=dtype).ravel(), int(lda)
+    a = np.asarray(a, dtype=dtype)
+    return np.asfortranarray(a).ravel(order="F"), a.shape[0]
+
+
+def _call_residual(lib_, prefix, kind, factor, original, ipiv, n, lda, pivoting, tile):
+    dt = factor.dtype
+    suffix = "f64" if dt == np.float64 else "f32"
+    err = ctypes.c_int(0)
+    if kind == "potrf":
+        f = getattr(lib_, f"{prefix}_potrf_residual_{suffix}")
+        r = f(_ptr(factor), _ptr(original), n, lda, tile, ctypes.byref(err))
+    else:
+        piv = None if ipiv is None else np.ascontiguousarray(ipiv, dtype=np.int32)
+        f = getattr(lib_, f"{prefix}_getrf_residual_{suffix}")
+        r = f(_ptr(factor), _ptr(original), _ptr(piv), n, lda, int(pivoting), tile,
+              ctypes.byref(err))
+    if err.value:
+        raise ValueError("invalid residual inputs")
+    return float(r)
+
+
+def potrf_residual(L, A, n, lda, tile=512, impl="oracle"):
+    """||A - L L^T||_F / ||A||_F in FP64 (flat column-major buffers with lda)."""
+    L = np.ascontiguousarray(L)
+    A = np.ascontiguousarray(A, dtype=L.dtype)
+    lib_ = lib() if impl == "oracle" else ref_lib()
+    return _call_residual(lib_, "oracle" if impl == "oracle" else "ref", "potrf",
+                          L, A, None, n, lda, False, tile)
+
+
+def getrf_residual(LU, A, ipiv, n, lda, pivoting=True, tile=512, impl="oracle"):
+    """||P A - L U||_F / ||A||_F in FP64; ipiv 1-based global LAPACK pivots."""
+    LU = np.ascontiguousarray(LU)
+    A = np.ascontiguousarray(A, dtype=LU.dtype)
+    lib_ = lib() if impl == "oracle" else ref_lib()
+    return _call_residual(lib_, "oracle" if impl == "oracle" else "ref", "getrf",
+                          LU, A, ipiv, n, lda, pivoting, tile)
+
+
+def scaled(residual: float, n: int) -> float:
+    """Residual scaled by n * eps32 (eps32 = 2**-23)."""
+    return residual / (n * EPS32)
+
+
+# --- BLAS-backed residuals (same definition, FP64 product by host BLAS) -----
+
+def _ssq_norm(x: np.ndarray) -> float:
+    if not np.all(np.isfinite(x)):
+        return float("inf")
+    s = np.max(np.abs(x)) if x.size else 0.0
+    if s == 0.0:
+        return 0.0
+    return float(s * np.sqrt(np.sum((x / s) ** 2)))
+
+
+def _ratio(num: float, den: float) -> float:
+    if not np.isfinite(num) or not np.isfinite(den):
+        return float("inf")
+    if den == 0.0:
+        return 0.0 if num == 0.0 else float("inf")
+    return num / den
+
+
+def potrf_residual_blas(L2d: np.ndarray, A2d: np.ndarray) -> float:
+    """2-D n x n arrays; uses the lower triangle of L2d."""
+    L = np.tril(np.asarray(L2d, dtype=np.float64))
+    A = np.asarray(A2d, dtype=np.float64)
+    R = L @ L.T - A
+    return _ratio(_ssq_norm(R), _ssq_norm(A))
+
+
+def ipiv_to_perm(ipiv, n):
+    perm = np.arange(n)
+    for r in range(n):
+        p = int(ipiv[r]) - 1
+        if p < r or p >= n:
+            return None
+        perm[r], perm[p] = perm[p], perm[r]
+    return perm
+
+
+def getrf_residual_blas(LU2d: np.ndarray, A2d: np.ndarray, ipiv) -> float:
+    n = LU2d.shape[0]
+    perm = ipiv_to_perm(ipiv, n)
+    if perm is None:
+        return float("inf")
+    LU = np.asarray(LU2d, dtype=np.float64)
+    L = np.tril(LU, -1) + np.eye(n)
+    U = np.triu(LU)
+    PA = np.asarray(A2d, dtype=np.float64)[perm, :]
+    return _ratio(_ssq_norm(L @ U - PA), _ssq_norm(PA))
+
+
+# --- reference loops restated in C (FP32) ----------------------------------
+
+def double_blocked_potrf(A2d: np.ndarray, nb: int, b: int, syrk_k_tile: int = 0):
+    A = np.asfortranarray(np.array(A2d, dtype=np.float32))
+    n = A.shape[0]
+    info = lib().oracle_double_blocked_potrf(A.ctypes.data_as(ctypes.c_void_p), n, n,
+                                             nb, b, syrk_k_tile)
+    return A, info
+
+
+def double_blocked_getrf(A2d: np.ndarray, outer_nb: int, inner_nb: int):
+    A = np.asfortranarray(np.array(A2d, dtype=np.float32))
+    n = A.shape[0]
+    ipiv = np.zeros(n, dtype=np.int32)
+    info = lib().oracle_double_blocked_getrf(A.ctypes.data_as(ctypes.c_void_p), n, n,
+                                             outer_nb, inner_nb,
+                                             ipiv.ctypes.data_as(ctypes.c_void_p))
+    return A, ipiv, info
+
+
+def parse_seed(text):
+    seed = ctypes.c_uint(19)
+    ok = lib().oracle_parse_seed(None if text is None else text.encode(), ctypes.byref(seed))
+    return bool(ok), seed.value
+
+
+# --- host LAPACK (SciPy OpenBLAS) -------------------------------------------
+
+def lapack_spotrf(A2d: np.ndarray):
+    from scipy.linalg import lapack
+    c, info = lapack.spotrf(np.asfortranarray(A2d, dtype=np.float32), lower=1,
+                            clean=0, overwrite_a=0)
+    return c, int(info)
+
+
+def lapack_sgetrf(A2d: np.ndarray):
+    """Returns (packed LU, 1-based ipiv, info) like LAPACK sgetrf."""
+    from scipy.linalg import lapack
+    lu, piv, info = lapack.sgetrf(np.asfortranarray(A2d, dtype=np.float32), overwrite_a=0)
+    return lu, (piv + 1).astype(np.int32), int(info)
+
+
+def lapack_dgetrf(A2d: np.ndarray):
+    from scipy.linalg import lapack
+    lu, piv, info = lapack.dgetrf(np.asfortranarray(A2d, dtype=np.float64), overwrite_a=0)
+    return lu, (piv + 1).astype(np.int32), int(info)
+
+
+# --- seeded generators (bit-identical to the device generator) --------------
+
+_M64 = (1 << 64) - 1
+_GOLD = np.uint64(0x9E3779B97F4A7C15)
+_MIX = np.uint64(0xD1B54A32D192ED03)
+
+
+def _splitmix(x: np.ndarray) -> np.ndarray:
+    x = x ^ (x >> np.uint64(30))
+    x = x * np.uint64(0xBF58476D1CE4E5B9)
+    x = x ^ (x >> np.uint64(27))
+    x = x * np.uint64(0x94D049BB133111EB)
+    x = x ^ (x >> np.uint64(31))
+    return x
+
+
+def uniform_pm1(count: int, seed: int, offset: int = 0) -> np.ndarray:
+    """Counter-based U[-1,1) FP32: element i = top-24-bit(h(seed, i)) / 2**23 - 1.
+
+    h(seed, i) = splitmix64_finalize(seed * 0x9E3779B97F4A7C15 + (i + 1) * 0xD1B54A32D192ED03)
+    (all mod 2**64).  Every value is a multiple of 2**-23 in [-1, 1), so it is
+    exact in FP32 and identical on host and device.
+    """
+    with np.errstate(over="ignore"):
+        idx = np.arange(offset, offset + count, dtype=np.uint64) + np.uint64(1)
+        x = np.uint64(seed) * _GOLD + idx * _MIX
+        x = _splitmix(x)
+    top = (x >> np.uint64(40)).astype(np.float64)
+    return (top / float(1 << 23) - 1.0).astype(np.float32)
+
+
+def general_uniform(n: int, seed: int) -> np.ndarray:
+    """n x n FP32 with iid U[-1,1) entries (column-major linear index)."""
+    return uniform_pm1(n * n, seed).reshape(n, n, order="F")
+
+
+def spd_gram(n: int, seed: int) -> np.ndarray:
+    """A = G G^T / n + I formed in FP64 then rounded to FP32 (G iid U[-1,1) FP32)."""
+    G = general_uniform(n, seed).astype(np.float64)
+    A = (G @ G.T) / n + np.eye(n)
+    A = 0.5 * (A + A.T)
+    return A.astype(np.float32)

@@ -1,0 +1,187 @@
+"""GPU parity tests for the pivoted LU path, called through the C ABI.
+
+Oracle: host LAPACK sgetrf (pivot sequences must be identical) and the C
+restatement of the reference's CPU FP64 residual (scaled by n * eps32, bound
+10); committed golden pivots in tests/golden/lapack_f32.npz."""
+import os
+
+import numpy as np
+import pytest
+
+import hygondoubleblockedfactorizations_b200 as hd_mod
+import oracle
+from tests.common import dev, getrf_check, host2d, info_tensor, padded, ptr
+
+pytestmark = pytest.mark.gpu
+
+BOUND = 10.0
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lapack_f32.npz")
+
+
+def run_getrf(hd, handle, torch, A2d, fn, lda=None, outer=0, inner=0, mode=0, tblock=0,
+              mtile=0, ws=None):
+    n = A2d.shape[0]
+    lda = lda or n
+    dA, _ = padded(torch, A2d, lda)
+    ipiv = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    info = info_tensor(torch)
+    h = handle.ptr
+    if fn == "double_blocked_getrf":
+        hd.call(fn, h, ptr(dA), lda, n, outer, inner, mode, tblock, ptr(ipiv), ptr(info))
+    elif fn == "double_blocked_getrf_batched_pivot":
+        hd.call(fn, h, ptr(dA), lda, n, outer, inner, mode, tblock, mtile, ptr(ipiv), ptr(info),
+                ws)
+    elif fn == "blocked_right_looking_getrf":
+        hd.call(fn, h, ptr(dA), lda, n, outer, ptr(ipiv), ptr(info))
+    elif fn == "double_blocked_getrf_npvt":
+        hd.call(fn, h, ptr(dA), lda, n, outer, inner, ptr(info))
+    elif fn == "blocked_right_looking_getrf_npvt":
+        hd.call(fn, h, ptr(dA), lda, n, outer, ptr(info))
+    torch.cuda.synchronize()
+    return dA, host2d(dA, lda, lda, n), ipiv.cpu().numpy()[:n], int(info.item())
+
+
+def make_ws(torch, n, tile=64):
+    keep = dict(src=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                tgt=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                swap=torch.zeros(n * tile, dtype=torch.float32, device="cuda"),
+                hp=np.zeros(n, np.int32), hperm=np.zeros(n, np.int32),
+                hs=np.zeros(n, np.int32), ht=np.zeros(n, np.int32))
+    ws = hd_mod.WorkspacePivot(keep["src"].data_ptr(), keep["tgt"].data_ptr(),
+                               keep["swap"].data_ptr(), keep["hp"].ctypes.data,
+                               keep["hperm"].ctypes.data, keep["hs"].ctypes.data,
+                               keep["ht"].ctypes.data, n, tile)
+    return ws, keep
+
+
+@pytest.mark.parametrize("n,outer,inner", [(512, 256, 64), (1024, 512, 128), (2048, 1024, 256)])
+def test_pivots_identical_to_lapack_immediate(hd, handle, torch_cuda, n, outer, inner):
+    G = oracle.general_uniform(n, 1)
+    _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf", outer=outer,
+                                  inner=inner)
+    handle.check()
+    assert handle.device_errors() == 0
+    _, ipiv_l, info_l = oracle.lapack_sgetrf(G)
+    assert info == info_l == 0
+    np.testing.assert_array_equal(ipiv, ipiv_l)
+    gold = np.load(GOLD)
+    np.testing.assert_array_equal(ipiv, gold[f"getrf_ipiv_{n}"])
+    assert getrf_check(LU[:n], G, ipiv) <= BOUND
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batched_pivot_variant(hd, handle, torch_cuda, mode):
+    import ctypes
+    n = 2048
+    G = oracle.general_uniform(n, 1)
+    ws, keep = make_ws(torch_cuda, n, tile=48)
+    _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf_batched_pivot",
+                                  outer=1024, inner=256, mode=mode, tblock=384, mtile=700,
+                                  ws=ctypes.byref(ws))
+    handle.check()
+    assert info == 0
+    gold = np.load(GOLD)
+    np.testing.assert_array_equal(ipiv, gold[f"getrf_ipiv_{n}"])
+    assert getrf_check(LU[:n], G, ipiv) <= BOUND
+
+
+def test_batched_pivot_invalid_workspace(hd, handle, torch_cuda):
+    import ctypes
+    n = 64
+    G = oracle.general_uniform(n, 1)
+    ws, keep = make_ws(torch_cuda, n)
+    ws.capacity = n - 1
+    _, _, _, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf_batched_pivot",
+                              outer=32, inner=16, ws=ctypes.byref(ws))
+    assert info == -1 and handle.last_status() != 0
+
+
+@pytest.mark.parametrize("n,outer,inner", [(1, 0, 0), (2, 1, 1), (33, 16, 8), (100, 64, 32),
+                                           (257, 128, 40), (600, 300, 100), (1000, 1000, 1000)])
+def test_ragged_sizes_and_padding(hd, handle, torch_cuda, n, outer, inner):
+    G = oracle.general_uniform(n, 5)
+    lda = n + 3
+    dA, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf", lda=lda,
+                                   outer=outer, inner=inner)
+    handle.check()
+    assert info == 0
+    assert np.all(np.isnan(LU[n:, :])), "padding rows written"
+    _, ipiv_l, _ = oracle.lapack_sgetrf(G)
+    np.testing.assert_array_equal(ipiv, ipiv_l)
+    assert getrf_check(LU[:n], G, ipiv) <= BOUND
+
+
+def test_right_looking_variant(hd, handle, torch_cuda):
+    n = 1536
+    G = oracle.general_uniform(n, 1)
+    _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "blocked_right_looking_getrf",
+                                  outer=192)
+    handle.check()
+    _, ipiv_l, _ = oracle.lapack_sgetrf(G)
+    np.testing.assert_array_equal(ipiv, ipiv_l)
+    assert info == 0 and getrf_check(LU[:n], G, ipiv) <= BOUND
+
+
+@pytest.mark.parametrize("fn", ["double_blocked_getrf_npvt", "blocked_right_looking_getrf_npvt"])
+def test_no_pivot_variants(hd, handle, torch_cuda, fn):
+    n = 1024
+    G = oracle.general_uniform(n, 1) + np.float32(n) * np.eye(n, dtype=np.float32)
+    _, LU, _, info = run_getrf(hd, handle, torch_cuda, G, fn, outer=512, inner=128)
+    handle.check()
+    assert info == 0
+    assert getrf_check(LU[:n], G, None, pivoting=False) <= BOUND
+    ref, _ = oracle.double_blocked_getrf(G, 512, 128)  # pivoting never triggers here
+    assert np.abs(LU[:n] - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
+def test_singular_info(hd, handle, torch_cuda):
+    """Exact zero pivot: info = first zero U(i,i) (LAPACK sgetrf)."""
+    n = 300
+    G = oracle.general_uniform(n, 9)
+    G[:, 77] = 0.0
+    _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf", outer=128,
+                                  inner=32)
+    _, ipiv_l, info_l = oracle.lapack_sgetrf(G)
+    assert info == info_l == 78
+    np.testing.assert_array_equal(ipiv[:77], ipiv_l[:77])
+
+
+def test_apply_panel_pivots_launcher(hd, handle, torch_cuda):
+    """launch_apply_getrf_panel_pivots vs the reference kernel's semantics."""
+    n, panel, size = 300, 40, 50
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((n, n)).astype(np.float32)
+    piv = np.array([rng.integers(o + 1, n - panel + 1) for o in range(size)], dtype=np.int32)
+    want = A.copy()
+    for c in range(n):
+        if panel <= c < panel + size:
+            continue
+        for o in range(size):
+            r, pr = panel + o, panel + piv[o] - 1
+            want[[r, pr], c] = want[[pr, r], c]
+    dA = dev(torch_cuda, A)
+    dp = dev(torch_cuda, piv)
+    stream = torch_cuda.cuda.current_stream().cuda_stream
+    hd.call("launch_apply_getrf_panel_pivots", ptr(dA), n, n, panel, size, ptr(dp), stream)
+    torch_cuda.cuda.synchronize()
+    np.testing.assert_array_equal(host2d(dA, n, n, n), want)
+    np.testing.assert_array_equal(dp.cpu().numpy(), piv + panel)
+
+
+def test_apply_permutation_launcher(hd, handle, torch_cuda):
+    n, cols, tile = 400, 37, 8
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((n, cols)).astype(np.float32)
+    rows = rng.choice(n, 60, replace=False).astype(np.int32)
+    src = rows.copy()
+    tgt = rng.permutation(rows).astype(np.int32)
+    want = A.copy()
+    want[tgt, :] = A[src, :]
+    dA = dev(torch_cuda, A)
+    ds, dt = dev(torch_cuda, src), dev(torch_cuda, tgt)
+    tmp = torch_cuda.zeros(60 * tile, dtype=torch_cuda.float32, device="cuda")
+    stream = torch_cuda.cuda.current_stream().cuda_stream
+    hd.call("launch_apply_getrf_permutation", ptr(dA), n, cols, ptr(ds), ptr(dt), 60, ptr(tmp),
+            tile, stream)
+    torch_cuda.cuda.synchronize()
+    np.testing.assert_array_equal(host2d(dA, n, n, cols), want)

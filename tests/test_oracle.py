@@ -1,0 +1,188 @@
+"""CPU tests of the oracle: the C restatement of the reference's FP64 residual
+pinned against the reference's own golden outputs and against the checks of
+tests/cpu_fp64_residual/test_cpu_fp64_residual.cpp (restated here)."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.golden.make_golden import RES_CASES, gen_case, residual
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+
+
+def test_residual_matches_reference_golden():
+    with open(os.path.join(GOLD, "residual_ref.json")) as f:
+        gold = json.load(f)
+    assert len(gold) == len(RES_CASES)
+    for g in gold:
+        c = {k: g[k] for k in ("n", "lda", "kind", "dtype", "tile", "seed")}
+        got = residual(c, "oracle")
+        want = g["value"]
+        if np.isinf(want):
+            assert np.isinf(got), c
+        else:
+            assert got == pytest.approx(want, rel=1e-12, abs=1e-300), c
+
+
+def test_residual_matches_reference_live():
+    """Same cases against the reference header compiled in place (when present)."""
+    if oracle.ref_lib() is None:
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    for c in RES_CASES[::7]:
+        a, b = residual(c, "oracle"), residual(c, "ref")
+        assert (np.isinf(a) and np.isinf(b)) or a == pytest.approx(b, rel=1e-12), c
+
+
+def _long_double_reference(factor, original, perm, n, lda, cholesky):
+    """Unblocked oracle (test_cpu_fp64_residual.cpp:25-49) in extended precision."""
+    num = np.longdouble(0)
+    den = np.longdouble(0)
+    F = np.asarray(factor, dtype=np.longdouble)
+    for j in range(n):
+        for i in range(n):
+            prod = np.longdouble(0)
+            for k in range(n):
+                left = 0 if i < k else (1 if (not cholesky and i == k) else F[k * lda + i])
+                if cholesky:
+                    right = 0 if j < k else F[k * lda + j]
+                else:
+                    right = 0 if k > j else F[j * lda + k]
+                prod += np.longdouble(left) * np.longdouble(right)
+            a = np.longdouble(original[j * lda + perm[i]])
+            num += (prod - a) ** 2
+            den += a * a
+    return float(np.sqrt(num / den))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 11])
+@pytest.mark.parametrize("padding", [0, 3])
+@pytest.mark.parametrize("cholesky,pivoting", [(False, False), (False, True), (True, False)])
+def test_layouts_tiles_permutation(n, padding, cholesky, pivoting):
+    """test_cpu_fp64_residual.cpp:51-107: layouts, lda padding, 3-cycle pivots, tiles."""
+    lda = n + padding
+    factor = np.full(lda * n, np.nan, dtype=np.float32)
+    original = np.zeros(lda * n, dtype=np.float32)
+    pivots = np.arange(1, n + 1, dtype=np.int32)
+    perm = list(range(n))
+    if pivoting and n >= 3:
+        pivots[0] = 3
+        pivots[1] = 3
+        for k in range(n):
+            p = pivots[k] - 1
+            perm[k], perm[p] = perm[p], perm[k]
+    for j in range(n):
+        for i in range(n):
+            if not cholesky or i >= j:
+                factor[j * lda + i] = np.float32(0.13) * np.float32(i + 1) - np.float32(0.07) * np.float32(j + 1) + (np.float32(2) if i == j else np.float32(0))
+    for j in range(n):
+        for i in range(n):
+            prod = np.longdouble(0)
+            for k in range(min(i, j) + 1):
+                l = 1.0 if (not cholesky and i == k) else factor[k * lda + i]
+                r = factor[k * lda + j] if cholesky else factor[j * lda + k]
+                prod += np.longdouble(l) * np.longdouble(r)
+            original[j * lda + perm[i]] = np.float32(prod)
+    expected = _long_double_reference(factor, original, perm, n, lda, cholesky)
+    for tile in (1, 2, 3, 4, 512):
+        if cholesky:
+            got = oracle.potrf_residual(factor, original, n, lda, tile)
+        else:
+            got = oracle.getrf_residual(factor, original, pivots, n, lda, pivoting, tile)
+        tol = max(1e-18, abs(expected) * 1e-7)
+        assert np.isfinite(got) and abs(got - expected) <= tol
+
+
+def test_precision_and_errors():
+    """test_cpu_fp64_residual.cpp:109-147."""
+    f = np.nextafter(np.float32(1), np.float32(2))
+    o = np.float32(f * f)
+    exact = np.longdouble(f) * np.longdouble(f)
+    r = oracle.potrf_residual(np.array([f]), np.array([o]), 1, 1)
+    assert r > 0
+    assert r == pytest.approx(float(abs(exact - np.longdouble(o)) / np.longdouble(o)), rel=1e-7)
+    z, one = np.array([0], np.float32), np.array([1], np.float32)
+    assert oracle.potrf_residual(z, z, 1, 1) == 0
+    assert np.isinf(oracle.potrf_residual(one, z, 1, 1))
+    assert np.isinf(oracle.potrf_residual(np.array([np.nan], np.float32), one, 1, 1))
+    assert np.isinf(oracle.getrf_residual(one, one, np.array([0], np.int32), 1, 1, True))
+    for tile in (0, -1):
+        with pytest.raises(ValueError):
+            oracle.potrf_residual(one, one, 1, 1, tile)
+    big = oracle.getrf_residual(np.array([1e160]), np.array([2e160]), None, 1, 1, False)
+    assert big == pytest.approx(0.5, rel=1e-7)
+    small = oracle.getrf_residual(np.array([1e-200]), np.array([2e-200]), None, 1, 1, False)
+    assert small == pytest.approx(0.5, rel=1e-7)
+
+
+def test_seed_parser():
+    """test_cpu_fp64_residual.cpp:149-165 (seed.h:5-19)."""
+    assert oracle.parse_seed("0") == (True, 0)
+    assert oracle.parse_seed("4294967295") == (True, 4294967295)
+    for text in ("", "-1", "+1", "1x", "4294967296"):
+        ok, v = oracle.parse_seed(text)
+        assert not ok and v == 19
+    assert not oracle.parse_seed(None)[0]
+
+
+def test_reference_unit_test_binary_passes():
+    """Run the reference's own 170-check test compiled in place (oracle/_ref)."""
+    exe = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "test_cpu_fp64_residual")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref not built")
+    p = subprocess.run([exe], capture_output=True, text=True)
+    assert p.returncode == 0 and "PASS: 170 checks" in p.stdout
+
+
+def test_blas_residual_agrees_with_c_oracle():
+    for n in (7, 33, 96):
+        A = oracle.spd_gram(n, 3)
+        L, info = oracle.double_blocked_potrf(A, 32, 8)
+        assert info == 0
+        a = oracle.potrf_residual(L.ravel(order="F"), np.asfortranarray(A).ravel(order="F"), n, n)
+        b = oracle.potrf_residual_blas(L, A)
+        assert a == pytest.approx(b, rel=1e-9)
+        G = oracle.general_uniform(n, 4)
+        LU, ipiv, info = oracle.double_blocked_getrf(G, 32, 8)
+        a = oracle.getrf_residual(LU.ravel(order="F"), G.ravel(order="F"), ipiv, n, n)
+        b = oracle.getrf_residual_blas(LU, G, ipiv)
+        assert a == pytest.approx(b, rel=1e-9)
+
+
+@pytest.mark.parametrize("n,nb,b", [(200, 64, 16), (300, 128, 32), (97, 40, 7)])
+def test_c_double_blocked_loops_match_lapack(n, nb, b):
+    """The reference schedules restated in C reproduce host LAPACK's pivots and
+    stay within the scaled-residual bound."""
+    A = oracle.spd_gram(n, 0)
+    L, info = oracle.double_blocked_potrf(A, nb, b, syrk_k_tile=nb // 2)
+    assert info == 0 and oracle.scaled(oracle.potrf_residual_blas(L, A), n) <= 10
+    G = oracle.general_uniform(n, 1)
+    LU, ipiv, info = oracle.double_blocked_getrf(G, nb, b)
+    _, ipiv_l, info_l = oracle.lapack_sgetrf(G)
+    assert info == info_l == 0
+    np.testing.assert_array_equal(ipiv, ipiv_l)
+    assert oracle.scaled(oracle.getrf_residual_blas(LU, G, ipiv), n) <= 10
+
+
+def test_lapack_golden_pivots_reproduce():
+    """Committed host-sgetrf pivots (tests/golden/lapack_f32.npz) match a live run."""
+    g = np.load(os.path.join(GOLD, "lapack_f32.npz"))
+    for n in (64, 256, 512):
+        _, ipiv, info = oracle.lapack_sgetrf(oracle.general_uniform(n, 1))
+        np.testing.assert_array_equal(ipiv, g[f"getrf_ipiv_{n}"])
+        assert g[f"getrf_scaled_{n}"] <= 10 and g[f"potrf_scaled_{n}"] <= 10
+
+
+def test_generator_values():
+    u = oracle.uniform_pm1(1 << 16, 7)
+    assert u.dtype == np.float32 and u.min() >= -1 and u.max() < 1
+    assert np.all((u.astype(np.float64) + 1) * 2 ** 23 == np.round((u.astype(np.float64) + 1) * 2 ** 23))
+    assert abs(float(u.mean())) < 0.01
+    np.testing.assert_array_equal(oracle.uniform_pm1(10, 7, offset=5), u[5:15])
+    A = oracle.spd_gram(64, 0)
+    np.testing.assert_array_equal(A, A.T)
+    assert np.linalg.eigvalsh(A.astype(np.float64)).min() > 0.9
