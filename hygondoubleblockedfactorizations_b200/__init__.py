@@ -42,6 +42,7 @@ _PROTOS = {
     "hdbf_profile_end": (c_int, [P, c_int, P, P, P, P]),
     "hdbf_profile_class_name": (ctypes.c_char_p, [c_int]),
     "hdbf_profile_num_classes": (c_int, []),
+    "hdbf_set_graph_mode": (c_int, [P, c_int]),
     # potrf
     "double_blocked_potrf": (None, [P, P, c_int, c_int, c_int, c_int, P]),
     "double_blocked_potrf_dbtrsm": (None, [P, P, c_int, c_int, c_int, c_int, P]),
@@ -151,6 +152,9 @@ class Handle:
         st = lib().hdbf_reserve_workspace(self._h, nbytes)
         if st != 0:
             raise HdbfError(f"reserve_workspace: {status_string(st)}")
+
+    def set_graphs(self, enabled: bool):
+        lib().hdbf_set_graph_mode(self._h, 1 if enabled else 0)
 
     def launches(self) -> int:
         return int(lib().hdbf_launch_count(self._h))

@@ -93,8 +93,10 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
 {
     if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
     if (mode != PivotMode::None && n > 0 && !ipiv) return HDBF_STATUS_INVALID_VALUE;
-    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
-    if (n == 0) return last_cuda(ctx);
+    if (n == 0) {
+        if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+        return last_cuda(ctx);
+    }
     GetrfWs ws;
     HDBF_TRY(getrf_workspace(ctx, n, &ws));
     if (mode == PivotMode::Batched && user_ws) {
@@ -107,7 +109,12 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
     if (inner_nb <= 0) inner_nb = outer_nb;
     inner_nb = std::min(inner_nb, outer_nb);
     const bool piv = mode != PivotMode::None;
-
+    const std::vector<long long> key = {
+        10 + (int)mode, (long long)A, lda, n, outer_nb, inner_nb, iterative_outer, trsm_block,
+        inner_gemm_m_tile, (long long)ipiv, (long long)info, (long long)ws.src, (long long)ws.tgt,
+        (long long)ws.temp, ws.temp_cols};
+    return run_graph(ctx, key, [&]() -> hdbf_status {
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int outer = 0; outer < n; outer += outer_nb) {
         const int oend = outer + std::min(outer_nb, n - outer);
         for (int inner = outer; inner < oend; inner += inner_nb) {
@@ -158,7 +165,8 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
                                at(A, lda, 0, next), lda, at(A, lda, next, next), lda));
         }
     }
-    return HDBF_STATUS_SUCCESS;
+    return last_cuda(ctx);
+    });
 }
 
 // Blocked right-looking LU (src/getrf/blocked_getrf.cpp:15-71).
@@ -167,11 +175,17 @@ hdbf_status getrf_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, i
 {
     if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
     if (piv && n > 0 && !ipiv) return HDBF_STATUS_INVALID_VALUE;
-    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
-    if (n == 0) return last_cuda(ctx);
+    if (n == 0) {
+        if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+        return last_cuda(ctx);
+    }
     GetrfWs ws;
     HDBF_TRY(getrf_workspace(ctx, n, &ws));
     if (nb <= 0) nb = n;
+    const std::vector<long long> key = {20 + (int)piv, (long long)A, lda, n, nb, (long long)ipiv,
+                                        (long long)info};
+    return run_graph(ctx, key, [&]() -> hdbf_status {
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int p = 0; p < n; p += nb) {
         const int psz = std::min(nb, n - p);
         const int next = p + psz;
@@ -189,7 +203,8 @@ hdbf_status getrf_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, i
                                at(A, lda, p, next), lda, at(A, lda, next, next), lda));
         }
     }
-    return HDBF_STATUS_SUCCESS;
+    return last_cuda(ctx);
+    });
 }
 
 bool batched_ws_valid(const getrf_batched_pivot_workspace* w, int n)

@@ -101,11 +101,18 @@ hdbf_status potrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, i
                           bool use_dbtrsm, int syrk_k_tile, int m_tile, int m_thr, int k_thr)
 {
     if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
-    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
-    if (n == 0) return last_cuda(ctx);
+    if (n == 0) {
+        if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+        return last_cuda(ctx);
+    }
+    HDBF_TRY(ensure_ws(ctx, n));
     if (nb <= 0) nb = n;
     if (b <= 0) b = nb;
     b = std::min(b, nb);
+    const std::vector<long long> key = {1, (long long)A, lda, n, nb, b, (long long)info,
+                                        use_dbtrsm, syrk_k_tile, m_tile, m_thr, k_thr};
+    return run_graph(ctx, key, [&]() -> hdbf_status {
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int outer = 0; outer < n; outer += nb) {
         const int oend = outer + std::min(nb, n - outer);
         for (int inner = outer; inner < oend; inner += b) {
@@ -143,16 +150,23 @@ hdbf_status potrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, i
                                at(A, lda, next, 0), lda, at(A, lda, below, next), lda));
         }
     }
-    return HDBF_STATUS_SUCCESS;
+    return last_cuda(ctx);
+    });
 }
 
 // src/potrf/blocked_potrf.cpp:126-178.
 hdbf_status potrf_blocked_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, int* info)
 {
     if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
-    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
-    if (n == 0) return last_cuda(ctx);
+    if (n == 0) {
+        if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+        return last_cuda(ctx);
+    }
+    HDBF_TRY(ensure_ws(ctx, n));
     if (nb <= 0) nb = n;
+    const std::vector<long long> key = {2, (long long)A, lda, n, nb, (long long)info};
+    return run_graph(ctx, key, [&]() -> hdbf_status {
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int k = 0; k < n; k += nb) {
         const int psz = std::min(nb, n - k);
         const int tr = n - k - psz;
@@ -163,7 +177,8 @@ hdbf_status potrf_blocked_rl_impl(hdbf_context* ctx, float* A, int lda, int n, i
         HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
         HDBF_TRY(syrk_lower(ctx, tr, psz, A21, lda, at(A, lda, k + psz, k + psz), lda));
     }
-    return HDBF_STATUS_SUCCESS;
+    return last_cuda(ctx);
+    });
 }
 
 // src/trsm/recursive_trsm.cpp:132-200: B (n x m) <- B * L^{-T}, split m.
@@ -231,6 +246,23 @@ hdbf_status rec_potrf_impl(hdbf_context* ctx, float* A, long long lda, int n, in
     return rec_potrf_impl(ctx, A22, lda, n2, nb, info, info_base + n1, tiled);
 }
 
+hdbf_status rec_potrf_entry(hdbf_context* ctx, float* A, int lda, int n, int nb, int* info,
+                            bool tiled)
+{
+    if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
+    if (n == 0) {
+        if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+        return last_cuda(ctx);
+    }
+    HDBF_TRY(ensure_ws(ctx, n));
+    const std::vector<long long> key = {3, (long long)A, lda, n, nb, (long long)info, tiled};
+    return run_graph(ctx, key, [&]() -> hdbf_status {
+        if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+        HDBF_TRY(rec_potrf_impl(ctx, A, lda, n, nb, info, 0, tiled));
+        return last_cuda(ctx);
+    });
+}
+
 }  // namespace
 }  // namespace hdbf
 
@@ -286,9 +318,7 @@ void recursive_potrf(hdbf_handle h, StreamPool* pool, float* A, int lda, int n, 
 {
     (void)pool;
     if (!h) return;
-    if (bad_matrix(A, lda, n)) { record(h, HDBF_STATUS_INVALID_VALUE); return; }
-    if (info) cudaMemsetAsync(info, 0, sizeof(int), h->stream);
-    record(h, rec_potrf_impl(h, A, lda, n, nb, info, 0, false));
+    record(h, rec_potrf_entry(h, A, lda, n, nb, info, false));
 }
 
 void recursive_potrf_tiled_trsm(hdbf_handle h, StreamPool* pool, float* A, int lda, int n,
@@ -296,9 +326,7 @@ void recursive_potrf_tiled_trsm(hdbf_handle h, StreamPool* pool, float* A, int l
 {
     (void)pool;
     if (!h) return;
-    if (bad_matrix(A, lda, n)) { record(h, HDBF_STATUS_INVALID_VALUE); return; }
-    if (info) cudaMemsetAsync(info, 0, sizeof(int), h->stream);
-    record(h, rec_potrf_impl(h, A, lda, n, nb, info, 0, true));
+    record(h, rec_potrf_entry(h, A, lda, n, nb, info, true));
 }
 
 void syrk_lower_update(hdbf_handle h, int n, int k, const float* A, int lda, float* C, int ldc)

@@ -35,32 +35,59 @@ hdbf_status potrf_diag(hdbf_context* ctx, int n, float* A, long long lda, int* i
     return potrf_diag(ctx, n2, A22, lda, info, info_base + n1);
 }
 
+namespace {
+// Recursive right/lower/transposed solve with precomputed 64x64 block inverses
+// (inv holds the blocks of L starting at block `blk`).
+hdbf_status trsm_rlt_rec(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
+                         float* B, long long ldb, const float* inv)
+{
+    if (cols <= kDiagLeaf) return rlt_apply(ctx, rows, cols, inv, B, ldb);
+    const int c1 = split_at(cols, kDiagLeaf);
+    const int c2 = cols - c1;
+    HDBF_TRY(trsm_rlt_rec(ctx, rows, c1, L, ldl, B, ldb, inv));
+    // B2 -= X1 * L21^T, L21 = L(c1:cols, 0:c1)
+    HDBF_TRY(sgemm_sub(ctx, false, false, rows, c2, c1, B, ldb, L + c1, ldl,
+                       B + (long long)c1 * ldb, ldb));
+    return trsm_rlt_rec(ctx, rows, c2, L + (long long)c1 * ldl + c1, ldl,
+                        B + (long long)c1 * ldb, ldb, inv + (long long)(c1 / kDiagLeaf) * 4096);
+}
+
+hdbf_status trsm_llu_rec(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
+                         float* B, long long ldb, const float* inv)
+{
+    if (rows <= kDiagLeaf) return llu_apply(ctx, rows, cols, inv, B, ldb);
+    const int r1 = split_at(rows, kDiagLeaf);
+    const int r2 = rows - r1;
+    HDBF_TRY(trsm_llu_rec(ctx, r1, cols, L, ldl, B, ldb, inv));
+    // B2 -= L21 * X1
+    HDBF_TRY(sgemm_sub(ctx, true, false, r2, cols, r1, L + r1, ldl, B, ldb, B + r1, ldb));
+    return trsm_llu_rec(ctx, r2, cols, L + (long long)r1 * ldl + r1, ldl, B + r1, ldb,
+                        inv + (long long)(r1 / kDiagLeaf) * 4096);
+}
+}  // namespace
+
+// B(rows x cols) <- B * L^{-T}: invert the 64x64 diagonal blocks of L once,
+// then recurse on column halves with GEMM updates; leaves are small GEMMs
+// with the inverted blocks (no serial dependency chains).
 hdbf_status trsm_rlt(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
                      float* B, long long ldb)
 {
     if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
-    if (cols <= kDiagLeaf) return trsm_rlt_small(ctx, rows, cols, L, ldl, B, ldb);
-    const int c1 = split_at(cols, kDiagLeaf);
-    const int c2 = cols - c1;
-    HDBF_TRY(trsm_rlt(ctx, rows, c1, L, ldl, B, ldb));
-    // B2 -= X1 * L21^T, L21 = L(c1:cols, 0:c1)
-    HDBF_TRY(sgemm_sub(ctx, false, false, rows, c2, c1, B, ldb, L + c1, ldl,
-                       B + (long long)c1 * ldb, ldb));
-    return trsm_rlt(ctx, rows, c2, L + (long long)c1 * ldl + c1, ldl, B + (long long)c1 * ldb,
-                    ldb);
+    HDBF_TRY(ensure_ws(ctx, cols));
+    float* inv = ws_inv(ctx);
+    HDBF_TRY(tri_inv64(ctx, cols, L, ldl, false, inv));
+    return trsm_rlt_rec(ctx, rows, cols, L, ldl, B, ldb, inv);
 }
 
+// B(rows x cols) <- L^{-1} B, L unit lower, same scheme on row halves.
 hdbf_status trsm_llu(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
                      float* B, long long ldb)
 {
     if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
-    if (rows <= kDiagLeaf) return trsm_llu_small(ctx, rows, cols, L, ldl, B, ldb);
-    const int r1 = split_at(rows, kDiagLeaf);
-    const int r2 = rows - r1;
-    HDBF_TRY(trsm_llu(ctx, r1, cols, L, ldl, B, ldb));
-    // B2 -= L21 * X1
-    HDBF_TRY(sgemm_sub(ctx, true, false, r2, cols, r1, L + r1, ldl, B, ldb, B + r1, ldb));
-    return trsm_llu(ctx, r2, cols, L + (long long)r1 * ldl + r1, ldl, B + r1, ldb);
+    HDBF_TRY(ensure_ws(ctx, rows));
+    float* inv = ws_inv(ctx);
+    HDBF_TRY(tri_inv64(ctx, rows, L, ldl, true, inv));
+    return trsm_llu_rec(ctx, rows, cols, L, ldl, B, ldb, inv);
 }
 
 hdbf_status syrk_lower(hdbf_context* ctx, int n, int k, const float* A, long long lda,
@@ -71,19 +98,11 @@ hdbf_status syrk_lower(hdbf_context* ctx, int n, int k, const float* A, long lon
 
 hdbf_status getrf_workspace(hdbf_context* ctx, int n, GetrfWs* ws)
 {
-    hdbf_status st;
-    const size_t need = hdbf_workspace_bytes_for(n);
-    char* base = static_cast<char*>(workspace(ctx, need, &st));
-    if (!base) return st;
-    size_t off = getf2_coop_scratch_bytes();  // the coop scratch sits at offset 0
-    const size_t ints = align_up(size_t(std::max(n, 1)) * sizeof(int), 256);
-    ws->src = reinterpret_cast<int*>(base + off);
-    off += ints;
-    ws->tgt = reinterpret_cast<int*>(base + off);
-    off += ints;
-    ws->gperm = reinterpret_cast<int*>(base + off);
-    off += ints;
-    ws->temp = reinterpret_cast<float*>(base + off);
+    HDBF_TRY(ensure_ws(ctx, n));
+    ws->src = ws_src(ctx);
+    ws->tgt = ws_tgt(ctx);
+    ws->gperm = ws_gperm(ctx);
+    ws->temp = ws_temp(ctx);
     ws->temp_cols = 64;
     ws->count = ctx->dev_small + kSmallMoveCount;
     return HDBF_STATUS_SUCCESS;

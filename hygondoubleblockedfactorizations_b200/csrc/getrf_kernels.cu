@@ -6,8 +6,8 @@
 // contiguous slice of rows of the block resident in shared memory; per column
 // the CTAs publish their local |max| candidate (value, row and the full
 // candidate row) and the owner of the diagonal row publishes that row, then
-// meet at one bounded grid barrier, after which every CTA picks the same
-// global winner (largest |a|, lowest row on ties -- LAPACK ISAMAX), swaps,
+// exchange them through global memory (see the protocol note below), after
+// which every CTA picks the same global winner (largest |a|, lowest row on ties -- LAPACK ISAMAX), swaps,
 // scales by the reciprocal pivot (division when |pivot| < FLT_MIN, as
 // xGETF2) and applies the rank-1 update to its own rows.
 //
@@ -27,8 +27,9 @@ namespace {
 
 constexpr int kCoopThreads = 256;
 constexpr int kCoopMaxW = 32;
-constexpr int kCoopMaxGrid = 1024;
-constexpr int kCandStride = kCoopMaxW + 2;  // |val|, row, w row values
+constexpr int kCoopMaxGrid = 256;
+// Per-(parity, CTA) exchange slot: [seq, |val|, row, pad | cand row (32) | diag row (32)]
+constexpr int kSlotFloats = 4 + 2 * kCoopMaxW;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
 {
@@ -42,38 +43,6 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Bounded sense-reversing grid barrier.  Returns false (and records a timeout
-// in *err) if the other CTAs did not arrive within the poll limit.
-__device__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err,
-                             int* s_ok)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned g = ld_acquire_u32(gen);
-        __threadfence();
-        const unsigned arrived = atomicAdd(count, 1u) + 1u;
-        if (arrived == nblocks) {
-            atomicExch(count, 0u);
-            __threadfence();
-            st_release_u32(gen, g + 1u);
-        } else {
-            unsigned polls = 0;
-            while (ld_acquire_u32(gen) == g) {
-                if (++polls > kSpinLimit) {
-                    ok = 0;
-                    atomicExch(err, kErrTimeout);
-                    break;
-                }
-                if (polls > 64) __nanosleep(64);
-            }
-        }
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
-
 // Candidate (v, i) beats (bv, bi): a real row beats none, then larger |a|,
 // then the lower row (LAPACK ISAMAX returns the first maximum).
 __device__ __forceinline__ bool better(float v, int i, float bv, int bi)
@@ -83,9 +52,19 @@ __device__ __forceinline__ bool better(float v, int i, float bv, int bi)
     return v > bv || (v == bv && i < bi);
 }
 
+// Exchange protocol (no grid barrier): for column j every CTA writes its slot
+// (parity j&1) -- candidate |max|, its row index and that row's w values, plus
+// the diagonal row j if it owns it -- then publishes seq = epoch*64 + j + 1
+// with a release store.  Every CTA polls all G seq words with acquire loads
+// (bounded), reduces the candidates identically, and fetches the winning row
+// and the old diagonal row.  A CTA can only overwrite a parity slot after all
+// CTAs have published the following column, i.e. after every CTA finished
+// reading that slot, so two parities suffice.  `epoch` is read at entry and
+// advanced by the last CTA to finish, so slots of earlier launches (and of
+// earlier CUDA-graph replays) never match.
 __global__ void __launch_bounds__(kCoopThreads)
 getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int ipiv_add,
-                  int* info, int info_base, float* scr, unsigned* bar_count, unsigned* bar_gen,
+                  int* info, int info_base, float* scr, unsigned* epoch_ptr, unsigned* done_ptr,
                   int* err, int pivot)
 {
     extern __shared__ float tile[];  // tile[c * rpc + r]
@@ -93,7 +72,9 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     __shared__ float orow[kCoopMaxW];
     __shared__ float red_v[kCoopThreads / 32];
     __shared__ int red_i[kCoopThreads / 32];
-    __shared__ int s_best_row, s_win_cta, s_ok;
+    __shared__ float cv[kCoopMaxGrid];
+    __shared__ int ci[kCoopMaxGrid];
+    __shared__ int s_best_row, s_win_cta, s_abort;
 
     const int G = gridDim.x;
     const int cta = blockIdx.x;
@@ -101,68 +82,91 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     const int lane = tid & 31, warp = tid >> 5;
     const int r0 = cta * rpc;
     const int nr = max(0, min(m, r0 + rpc) - r0);
+    const unsigned epoch = *reinterpret_cast<volatile unsigned*>(epoch_ptr);
 
     for (int c = 0; c < w; ++c)
         for (int r = tid; r < nr; r += kCoopThreads)
             tile[c * rpc + r] = A[(long long)c * lda + (r0 + r)];
+    if (tid == 0) s_abort = 0;
     __syncthreads();
 
-    float* cand_base = scr;                                   // [2][G][kCandStride]
-    float* diag_base = scr + 2 * kCoopMaxGrid * kCandStride;  // [2][kCoopMaxW]
     const int steps = min(m, w);
-    bool alive = true;
+    for (int j = 0; j < steps; ++j) {
+        const int par = j & 1;
+        const unsigned seq = (epoch << 6) + (unsigned)j + 1u;
+        float* slot = scr + ((long long)par * kCoopMaxGrid + cta) * kSlotFloats;
+        const int owner = j / rpc;
 
-    for (int j = 0; j < steps && alive; ++j) {
-        // Local candidate: largest |a(r, j)| over owned rows r >= j, lowest row on ties.
+        // 1. local candidate over owned rows >= j (largest |a|, lowest row)
         float bv = -1.f;
         int bi = INT_MAX;
-        for (int r = tid; pivot && r < nr; r += kCoopThreads) {
-            const int gr = r0 + r;
-            if (gr >= j) {
-                const float v = fabsf(tile[j * rpc + r]);
-                if (bi == INT_MAX || v > bv) { bv = v; bi = gr; }
+        if (pivot) {
+            for (int r = tid; r < nr; r += kCoopThreads) {
+                const int gr = r0 + r;
+                if (gr >= j) {
+                    const float v = fabsf(tile[j * rpc + r]);
+                    if (bi == INT_MAX || v > bv) { bv = v; bi = gr; }
+                }
             }
-        }
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const float ov = __shfl_down_sync(0xffffffffu, bv, off);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-            if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ov = __shfl_down_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+            }
+            if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+            __syncthreads();
+            if (tid == 0) {
+                for (int q = 1; q < kCoopThreads / 32; ++q)
+                    if (better(red_v[q], red_i[q], bv, bi)) { bv = red_v[q]; bi = red_i[q]; }
+                s_best_row = bi;
+                red_v[0] = bv;
+            }
+            __syncthreads();
         }
-        if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+
+        // 2. publish
+        const int my_best = pivot ? s_best_row : INT_MAX;
+        if (tid < w) {
+            if (my_best != INT_MAX) slot[4 + tid] = tile[tid * rpc + (my_best - r0)];
+            if (cta == owner) slot[4 + kCoopMaxW + tid] = tile[tid * rpc + (j - r0)];
+        }
+        if (tid == 0) {
+            slot[1] = pivot ? red_v[0] : -1.f;
+            slot[2] = __int_as_float(my_best);
+        }
         __syncthreads();
         if (tid == 0) {
-            for (int q = 1; q < kCoopThreads / 32; ++q)
-                if (better(red_v[q], red_i[q], bv, bi)) { bv = red_v[q]; bi = red_i[q]; }
-            s_best_row = bi;
+            __threadfence();
+            st_release_u32(reinterpret_cast<unsigned*>(slot), seq);
+        }
+
+        // 3. poll every slot (thread q watches CTA q), bounded
+        for (int q = tid; q < G; q += kCoopThreads) {
+            const float* sq = scr + ((long long)par * kCoopMaxGrid + q) * kSlotFloats;
+            unsigned polls = 0;
+            while (ld_acquire_u32(reinterpret_cast<const unsigned*>(sq)) != seq) {
+                if (++polls > kSpinLimit) {
+                    atomicExch(err, kErrTimeout);
+                    s_abort = 1;
+                    break;
+                }
+                if (polls > 256) __nanosleep(32);
+            }
+            cv[q] = __ldcg(sq + 1);
+            ci[q] = __float_as_int(__ldcg(sq + 2));
         }
         __syncthreads();
-        const int par = j & 1;
-        float* cand = cand_base + ((long long)par * kCoopMaxGrid + cta) * kCandStride;
-        const int my_best = s_best_row;
-        if (tid == 0) {
-            cand[0] = bv;
-            cand[1] = __int_as_float(my_best);
-        }
-        if (tid < w && my_best != INT_MAX) cand[2 + tid] = tile[tid * rpc + (my_best - r0)];
-        float* drow = diag_base + par * kCoopMaxW;
-        if (j >= r0 && j < r0 + nr && tid < w) drow[tid] = tile[tid * rpc + (j - r0)];
+        if (s_abort) break;
 
-        if (!grid_barrier(bar_count, bar_gen, (unsigned)G, err, &s_ok)) { alive = false; break; }
-
-        // Global winner (identical on every CTA); without pivoting the
-        // diagonal row is the pivot row.
+        // 4. global winner, identical on every CTA
         if (!pivot) {
             if (tid == 0) { s_best_row = j; s_win_cta = -1; }
         } else if (warp == 0) {
             float gv = -1.f;
             int gi = INT_MAX, gc = 0;
-            for (int q = lane; q < G; q += 32) {
-                const float* cq = cand_base + ((long long)par * kCoopMaxGrid + q) * kCandStride;
-                const float v = __ldcg(cq);
-                const int i = __float_as_int(__ldcg(cq + 1));
-                if (better(v, i, gv, gi)) { gv = v; gi = i; gc = q; }
-            }
+            for (int q = lane; q < G; q += 32)
+                if (better(cv[q], ci[q], gv, gi)) { gv = cv[q]; gi = ci[q]; gc = q; }
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
                 const float ov = __shfl_down_sync(0xffffffffu, gv, off);
@@ -175,41 +179,37 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         __syncthreads();
         const int p = s_best_row;
         if (tid < w) {
-            orow[tid] = __ldcg(drow + tid);
+            const float* so = scr + ((long long)par * kCoopMaxGrid + owner) * kSlotFloats;
+            orow[tid] = __ldcg(so + 4 + kCoopMaxW + tid);
             if (s_win_cta >= 0) {
-                const float* cw =
-                    cand_base + ((long long)par * kCoopMaxGrid + s_win_cta) * kCandStride;
-                prow[tid] = __ldcg(cw + 2 + tid);
+                const float* sw = scr + ((long long)par * kCoopMaxGrid + s_win_cta) * kSlotFloats;
+                prow[tid] = __ldcg(sw + 4 + tid);
             } else {
                 prow[tid] = orow[tid];
             }
         }
         if (pivot && cta == 0 && tid == 0) ipiv[j] = p + 1 + ipiv_add;
         __syncthreads();
+
+        // 5. swap rows j and p (within this column block), scale, rank-1 update
         if (p != j && tid < w) {
             if (j >= r0 && j < r0 + nr) tile[tid * rpc + (j - r0)] = prow[tid];
             if (p >= r0 && p < r0 + nr) tile[tid * rpc + (p - r0)] = orow[tid];
         }
         __syncthreads();
         const float piv = prow[j];
-        if (piv != 0.f) {
-            const bool recip = fabsf(piv) >= FLT_MIN;
-            const float rcp = 1.0f / piv;
-            for (int r = tid; r < nr; r += kCoopThreads) {
-                if (r0 + r > j) {
-                    float l = tile[j * rpc + r];
+        const bool nz = piv != 0.f;
+        const bool recip = fabsf(piv) >= FLT_MIN;
+        const float rcp = 1.0f / piv;
+        if (!nz && cta == 0 && tid == 0 && info) atomicCAS(info, 0, info_base + j + 1);
+        for (int r = tid; r < nr; r += kCoopThreads) {
+            if (r0 + r > j) {
+                float l = tile[j * rpc + r];
+                if (nz) {
                     l = recip ? l * rcp : l / piv;
                     tile[j * rpc + r] = l;
-                    for (int c = j + 1; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
                 }
-            }
-        } else {
-            if (cta == 0 && tid == 0 && info) atomicCAS(info, 0, info_base + j + 1);
-            for (int r = tid; r < nr; r += kCoopThreads) {
-                if (r0 + r > j) {
-                    const float l = tile[j * rpc + r];
-                    for (int c = j + 1; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
-                }
+                for (int c = j + 1; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
             }
         }
         __syncthreads();
@@ -218,6 +218,17 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     for (int c = 0; c < w; ++c)
         for (int r = tid; r < nr; r += kCoopThreads)
             A[(long long)c * lda + (r0 + r)] = tile[c * rpc + r];
+
+    // Advance the epoch once every CTA is done (the kernel's last action).
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        const unsigned done = atomicAdd(done_ptr, 1u) + 1u;
+        if (done == (unsigned)G) {
+            atomicExch(done_ptr, 0u);
+            atomicAdd(epoch_ptr, 1u);
+        }
+    }
 }
 
 // ------------------------------------------------------------ compose swaps
@@ -347,10 +358,24 @@ __global__ void scatter_rows_kernel(float* A, long long lda, int ncols,
 
 }  // namespace
 
+// Dynamic shared-memory opt-ins, set once per handle creation (never inside a
+// stream capture).
+void configure_getrf_kernels(hdbf_context* ctx)
+{
+    const size_t cap8 = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
+    const size_t cap4 = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
+    cudaFuncSetAttribute(getf2_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)cap8);
+    cudaFuncSetAttribute(compose_swaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)cap4);
+    cudaFuncSetAttribute(apply_moves_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)cap4);
+    cudaGetLastError();
+}
+
 size_t getf2_coop_scratch_bytes()
 {
-    return align_up((size_t)(2 * kCoopMaxGrid * kCandStride + 2 * kCoopMaxW) * sizeof(float),
-                    256);
+    return align_up((size_t)(2 * kCoopMaxGrid * kSlotFloats) * sizeof(float), 256);
 }
 
 hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
@@ -359,32 +384,26 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     int piv_flag = pivot ? 1 : 0;
     if (m <= 0 || w <= 0) return HDBF_STATUS_SUCCESS;
     if (w > kCoopMaxW) return HDBF_STATUS_INVALID_VALUE;
-    hdbf_status st;
-    float* scr = static_cast<float*>(workspace(ctx, getf2_coop_scratch_bytes(), &st));
-    if (!scr) return st;
+    HDBF_TRY(ensure_ws(ctx, 64));
+    float* scr = ws_coop(ctx);
 
-    // Grid: about 256 rows per CTA, at most one CTA per SM (co-residency is
-    // guaranteed by the cooperative launch), shared slice <= max opt-in.
-    static int occ_cached = -1;
+    // Grid: ~512 rows per CTA (fewer CTAs = fewer slots to poll per column),
+    // at most one CTA per SM; co-residency is guaranteed by the cooperative
+    // launch, which fails instead of hanging if the grid cannot fit.
     const size_t smem_cap = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
-    int G = (m + 255) / 256;
+    int G = (m + 511) / 512;
     if (G > ctx->sm_count) G = ctx->sm_count;
     if (G > kCoopMaxGrid) G = kCoopMaxGrid;
     if (G < 1) G = 1;
     int rpc = (m + G - 1) / G;
     size_t smem = (size_t)rpc * w * sizeof(float);
     if (smem > smem_cap) return HDBF_STATUS_NOT_SUPPORTED;
-    if (occ_cached < 0) {
-        cudaFuncSetAttribute(getf2_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_cap);
-        occ_cached = 1;
-    }
-    unsigned* bar_count = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallBarCount);
-    unsigned* bar_gen = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallBarGen);
+    unsigned* epoch = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallEpoch);
+    unsigned* done = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallDone);
     int* err = ctx->dev_small + kSmallErr;
     ProfScope prof(ctx, kClsPanel, (double)m * w * w - (double)w * w * w / 3.0, 8.0 * m * w);
     void* args[] = {&m, &w, &A, &lda, &rpc, &ipiv, &ipiv_add, &info, &info_base,
-                    &scr, &bar_count, &bar_gen, &err, &piv_flag};
+                    &scr, &epoch, &done, &err, &piv_flag};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)getf2_coop_kernel, dim3(G),
                                                 dim3(kCoopThreads), args, smem, ctx->stream);
     ctx->launches++;
@@ -402,12 +421,6 @@ hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_mi
     const size_t smem = (size_t)m * sizeof(int);
     const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
     const int use_smem = smem <= cap ? 1 : 0;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(compose_swaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)cap);
-        configured = true;
-    }
     if (!use_smem && !gperm) return HDBF_STATUS_INVALID_VALUE;
     ProfScope prof(ctx, kClsCompose, 0.0, 4.0 * k + 8.0 * m);
     compose_swaps_kernel<<<1, kComposeThreads, use_smem ? smem : 0, ctx->stream>>>(
@@ -424,13 +437,6 @@ hdbf_status apply_moves(hdbf_context* ctx, float* A, long long lda, int ncols,
     if (ncols <= 0 || max_moves <= 0) return HDBF_STATUS_SUCCESS;
     const size_t per_col = (size_t)max_moves * sizeof(float);
     const size_t budget = 48 * 1024;
-    static bool configured = false;
-    if (!configured) {
-        const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
-        cudaFuncSetAttribute(apply_moves_smem_kernel,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
-        configured = true;
-    }
     const size_t hard_cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
     ProfScope prof(ctx, kClsMoves, 0.0, 8.0 * (double)max_moves * ncols);
     if (per_col <= hard_cap) {

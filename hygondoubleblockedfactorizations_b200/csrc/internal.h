@@ -18,14 +18,24 @@ enum KernelClass {
     kClsPanel = 4,    // getf2_coop_kernel
     kClsCompose = 5,  // compose_swaps_kernel
     kClsMoves = 6,    // apply_moves kernels
-    kClsOther = 7,
-    kNumClasses = 8
+    kClsTrsmInv = 7,  // tri_inv64_kernel
+    kClsOther = 8,
+    kNumClasses = 9
 };
 struct ProfRec {
     int cls;
     cudaEvent_t a, b;
     double flops;
     double bytes;
+    int m = 0, n = 0, k = 0;  // problem shape (GEMM launches)
+};
+struct GraphEntry {
+    std::vector<long long> key;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<ProfRec> prof;  // event pairs baked into the graph (profiling graphs)
+    unsigned long long id = 0;
+    unsigned long long last_use = 0;
+    unsigned long long kernels = 0;  // kernel launches recorded in the graph
 };
 }  // namespace hdbf
 
@@ -37,6 +47,7 @@ struct hdbf_context {
     // Workspace arena (grown on demand outside stream capture).
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    int ws_n = 0;  // largest order whose layout fits in ws_bytes
     // Small always-present device block: [0] error word, [1..] barrier words.
     int* dev_small = nullptr;
     hdbf_status last_status = HDBF_STATUS_SUCCESS;
@@ -44,8 +55,13 @@ struct hdbf_context {
     // Optional per-launch event profiling.
     bool profiling = false;
     std::vector<hdbf::ProfRec> prof;
-    std::vector<cudaEvent_t> ev_pool;
-    size_t ev_used = 0;
+    // CUDA-graph cache of whole factorizations (key = entry point + arguments).
+    bool use_graphs = true;
+    bool capturing = false;
+    cudaStream_t cap_stream = nullptr;
+    std::vector<hdbf::GraphEntry> graphs;
+    unsigned long long graph_clock = 0;
+    std::vector<unsigned long long> prof_graph_ids;  // graphs replayed while profiling
 };
 
 struct hdbf_stream_pool {
@@ -57,9 +73,9 @@ namespace hdbf {
 
 // Layout of hdbf_context::dev_small (ints).
 constexpr int kSmallErr = 0;       // device error word (timeouts, invalid pivots)
-constexpr int kSmallBarCount = 4;  // grid-barrier arrive counter
-constexpr int kSmallBarGen = 8;    // grid-barrier generation
 constexpr int kSmallMoveCount = 12;  // move count of the last composed permutation
+constexpr int kSmallEpoch = 16;      // panel-kernel exchange epoch
+constexpr int kSmallDone = 20;       // panel-kernel finished-CTA counter
 constexpr int kSmallInts = 64;
 
 // Device error codes written into dev_small[kSmallErr].
@@ -75,7 +91,8 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // ctx->stream and records its class and algorithmic work.
 class ProfScope {
 public:
-    ProfScope(hdbf_context* ctx, int cls, double flops, double bytes = 0.0);
+    ProfScope(hdbf_context* ctx, int cls, double flops, double bytes = 0.0, int m = 0,
+              int n = 0, int k = 0);
     ~ProfScope();
 private:
     hdbf_context* ctx_;
@@ -85,6 +102,24 @@ private:
 // Make sure the workspace holds at least `bytes`; returns nullptr and sets
 // *st on failure.  Growing frees the old buffer (device-synchronising).
 void* workspace(hdbf_context* ctx, size_t bytes, hdbf_status* st);
+
+// Workspace layout for problems of order <= n (byte offsets):
+//   coop  panel-kernel exchange slots (fixed size, offset 0)
+//   inv   inverted 64x64 diagonal blocks, n*64 floats
+//   src, tgt, gperm  composed row moves / permutation scratch, n ints each
+//   temp  column-tiled swap buffer, 64*n floats
+struct WsLayout {
+    size_t coop, inv, src, tgt, gperm, temp, total;
+};
+WsLayout ws_layout(int n);
+// Guarantee the layout for order n (grows the arena outside stream capture).
+hdbf_status ensure_ws(hdbf_context* ctx, int n);
+float* ws_coop(hdbf_context* ctx);
+float* ws_inv(hdbf_context* ctx);
+int* ws_src(hdbf_context* ctx);
+int* ws_tgt(hdbf_context* ctx);
+int* ws_gperm(hdbf_context* ctx);
+float* ws_temp(hdbf_context* ctx);
 
 hdbf_status last_cuda(hdbf_context* ctx);
 
@@ -102,18 +137,23 @@ hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N,
 hdbf_status potf2_small(hdbf_context* ctx, int n, float* A, long long lda, int* info,
                         int info_base);
 
-// B(rows x cols) <- B * L^{-T}, L lower non-unit, cols <= 64.
-hdbf_status trsm_rlt_small(hdbf_context* ctx, int rows, int cols, const float* L,
-                           long long ldl, float* B, long long ldb);
-// B(rows x cols) <- L^{-1} B, L unit lower, rows <= 64.
-hdbf_status trsm_llu_small(hdbf_context* ctx, int rows, int cols, const float* L,
-                           long long ldl, float* B, long long ldb);
+// Inverses of the 64x64 diagonal blocks of lower-triangular L (order n) into
+// out[b*4096 ...] (column-major blocks); unit selects an implicit unit diagonal.
+hdbf_status tri_inv64(hdbf_context* ctx, int n, const float* L, long long ldl, bool unit,
+                      float* out);
+// Leaf applications of a precomputed block inverse (in place):
+// B(rows<=64 x cols) <- inv * B  and  B(rows x cols<=64) <- B * inv^T.
+hdbf_status llu_apply(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
+                      long long ldb);
+hdbf_status rlt_apply(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
+                      long long ldb);
 
 // Cooperative partially pivoted LU of an m x w panel (w <= 32).  Pivots are
 // written 1-based as (local row + 1 + ipiv_add).
 hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
                        int ipiv_add, int* info, int info_base, bool pivot);
 size_t getf2_coop_scratch_bytes();
+void configure_getrf_kernels(hdbf_context* ctx);
 
 // Compose LAPACK swaps  row (i) <-> row (ipiv[i]-1-ipiv_minus), i in [0,k),
 // over local rows [0, m) into (src, tgt, *count) moves.
@@ -150,6 +190,37 @@ struct GetrfWs {
 hdbf_status getrf_workspace(hdbf_context* ctx, int n, GetrfWs* ws);
 hdbf_status getrf_panel(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
                         int ipiv_add, int* info, int info_base, bool pivot, const GetrfWs& ws);
+
+// ---------------------------------------------------------------- graphs
+// A whole factorization is a long chain of dependent launches; replaying it
+// as one CUDA graph removes the per-launch host cost.  The first call with a
+// given key records the work on a private capture stream; later calls with
+// the same key replay the instantiated graph on the caller's stream.  The
+// workspace must already be reserved (no allocation may happen inside).
+GraphEntry* graph_find(hdbf_context* ctx, const std::vector<long long>& key);
+bool graph_can_capture(hdbf_context* ctx);
+hdbf_status graph_capture_begin(hdbf_context* ctx, cudaStream_t* saved);
+hdbf_status graph_capture_end(hdbf_context* ctx, cudaStream_t saved, hdbf_status body_status,
+                              const std::vector<long long>& key, size_t prof_mark,
+                              unsigned long long launches_before);
+hdbf_status graph_launch(hdbf_context* ctx, GraphEntry* e);
+void graph_cache_clear(hdbf_context* ctx);
+
+template <class Body>
+hdbf_status run_graph(hdbf_context* ctx, std::vector<long long> key, Body&& body)
+{
+    if (!graph_can_capture(ctx)) return body();
+    key.push_back(ctx->profiling ? 1 : 0);
+    if (GraphEntry* e = graph_find(ctx, key)) return graph_launch(ctx, e);
+    cudaStream_t saved = nullptr;
+    const size_t mark = ctx->prof.size();
+    const unsigned long long l0 = ctx->launches;
+    if (graph_capture_begin(ctx, &saved) != HDBF_STATUS_SUCCESS) return body();
+    const hdbf_status st = body();
+    const hdbf_status ge = graph_capture_end(ctx, saved, st, key, mark, l0);
+    if (ge == HDBF_STATUS_NOT_SUPPORTED) return body();  // capture refused: run eagerly
+    return ge;
+}
 
 }  // namespace hdbf
 

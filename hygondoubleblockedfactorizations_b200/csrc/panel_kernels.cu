@@ -2,8 +2,8 @@
 //
 // potf2_small replaces rocsolver_spotrf on the diagonal block
 // (src/potrf/double_blocked_potrf.cpp:34-56, call :334) at the leaf of this
-// library's recursive diagonal factorization; trsm_*_small replace
-// rocblas_strsm at the leaves of the recursive TRSMs
+// library's recursive diagonal factorization; tri_inv64 + {llu,rlt}_apply
+// replace rocblas_strsm at the leaves of the recursive TRSMs
 // (src/trsm/right_lower_trsm.cpp:24-37, src/getrf/getrf_npvt_internal.h:57-70).
 #include <cfloat>
 
@@ -14,140 +14,191 @@ namespace {
 
 constexpr int kLeaf = 64;
 
-// Right-looking Cholesky of an n x n (n <= 64) lower block held in shared
-// memory.  Pivot test and info follow LAPACK xPOTRF: the first column whose
-// updated diagonal is not > 0 (or is NaN) stops the factorization, its value
-// is left in place, and info = info_base + j + 1 (first failure wins).  A
-// block whose info is already non-zero is left untouched.
+// Right-looking Cholesky of an n x n (n <= 64) lower block, register
+// resident: thread (r, g) = (tid % 64, tid / 64) holds A(r, g + 4i), i < 16.
+// Per column j the owner group publishes the scaled column to shared memory
+// and every thread applies the rank-1 update to its own 16 entries (two
+// barriers per column, no shared-memory read-modify-write chains).
+// Pivot test and info follow LAPACK xPOTRF: the first column whose updated
+// diagonal is not > 0 (or is NaN) stops the factorization, its value is left
+// in place, and info = info_base + j + 1 (first failure wins).  A block whose
+// info is already non-zero is left untouched.
 __global__ void __launch_bounds__(256) potf2_kernel(int n, float* A, long long lda, int* info,
                                                     int info_base)
 {
-    __shared__ float s[kLeaf][kLeaf + 1];  // s[col][row]
-    __shared__ float s_diag;
+    __shared__ float lcol[kLeaf];
+    __shared__ float s_d;
     const int tid = threadIdx.x;
+    const int r = tid & 63;
+    const int g = tid >> 6;
     if (info && *reinterpret_cast<volatile int*>(info) != 0) return;
 
-    for (int idx = tid; idx < n * n; idx += blockDim.x) {
-        const int c = idx / n, r = idx - c * n;
-        if (r >= c) s[c][r] = A[(long long)c * lda + r];
+    float a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = g + 4 * i;
+        a[i] = (r < n && c < n && r >= c) ? A[(long long)c * lda + r] : 0.f;
     }
-    __syncthreads();
 
     int failed_at = -1;
     for (int j = 0; j < n; ++j) {
-        const float d = s[j][j];
+        const int gj = j & 3, ij = j >> 2;
+        float own = 0.f;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (i == ij) own = a[i];
+        if (g == gj && r == j) s_d = own;
         __syncthreads();
+        const float d = s_d;
         if (!(d > 0.f)) {  // uniform: every thread read the same value
             failed_at = j;
             break;
         }
         const float sd = sqrtf(d);
         const float rcp = 1.0f / sd;
-        if (tid == 0) s[j][j] = sd;
-        for (int i = j + 1 + tid; i < n; i += blockDim.x) s[j][i] *= rcp;
-        __syncthreads();
-        // trailing lower update: s[c][r] -= s[j][r] * s[j][c], j < c <= r
-        const int tc = tid >> 6, tr = tid & 63;
-        for (int c = j + 1 + tc; c < n; c += 4) {
-            const float ljc = s[j][c];
-            for (int r = c + tr; r < n; r += 64) s[c][r] -= s[j][r] * ljc;
+        if (g == gj) {
+            const float v = (r == j) ? sd : (r > j ? own * rcp : own);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (i == ij) a[i] = v;
+            if (r > j) lcol[r] = v;
         }
         __syncthreads();
+        if (r > j) {
+            const float lr = lcol[r];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int c = g + 4 * i;
+                if (c > j && c <= r) a[i] = fmaf(-lr, lcol[c], a[i]);
+            }
+        }
     }
 
-    for (int idx = tid; idx < n * n; idx += blockDim.x) {
-        const int c = idx / n, r = idx - c * n;
-        if (r >= c) A[(long long)c * lda + r] = s[c][r];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = g + 4 * i;
+        if (r < n && c < n && r >= c) A[(long long)c * lda + r] = a[i];
     }
     if (failed_at >= 0 && tid == 0 && info) atomicCAS(info, 0, info_base + failed_at + 1);
 }
 
-// B(rows x cols) <- B * L^{-T} (cols <= 64): one thread per row, the row held
-// in registers, L broadcast from shared memory.  Column order and the
-// reciprocal-of-diagonal scaling follow reference BLAS xTRSM (Right, Lower,
-// Transposed, Non-unit).
-constexpr int kRltThreads = 128;
-__global__ void __launch_bounds__(kRltThreads) trsm_rlt_kernel(int rows, int cols,
-                                                               const float* __restrict__ L,
-                                                               long long ldl, float* B,
-                                                               long long ldb)
+
+// Inverses of the 64x64 diagonal blocks of a lower-triangular n x n matrix
+// (unit or non-unit diagonal), one CTA per block, thread t solving
+// L_bb x = e_t by forward substitution (right-looking, so every L read is a
+// shared-memory broadcast).  out[b*4096 + c*64 + r] = inv(L_bb)(r, c); a
+// partial last block is padded with the identity.
+__global__ void __launch_bounds__(kLeaf) tri_inv64_kernel(int n, const float* __restrict__ L,
+                                                          long long ldl, int unit, float* out)
 {
-    __shared__ float Ls[kLeaf][kLeaf];  // Ls[c][r] = L(r, c)
-    __shared__ float rd[kLeaf];
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < kLeaf * kLeaf; idx += blockDim.x) {
+    __shared__ float Ls[kLeaf][kLeaf + 1];  // Ls[r][c] = L(base + r, base + c)
+    const int base = blockIdx.x * kLeaf;
+    const int nb = min(kLeaf, n - base);
+    const int t = threadIdx.x;
+    for (int idx = t; idx < kLeaf * kLeaf; idx += kLeaf) {
         const int c = idx / kLeaf, r = idx - c * kLeaf;
-        Ls[c][r] = (r < cols && c < cols && r >= c) ? L[(long long)c * ldl + r] : 0.f;
+        Ls[r][c] = (r < nb && c < nb && r >= c) ? L[(long long)(base + c) * ldl + base + r] : 0.f;
     }
     __syncthreads();
-    for (int c = tid; c < kLeaf; c += blockDim.x) rd[c] = (c < cols) ? 1.0f / Ls[c][c] : 0.f;
-    __syncthreads();
-
-    const long long row = (long long)blockIdx.x * kRltThreads + tid;
-    if (row >= rows) return;
     float x[kLeaf];
 #pragma unroll
-    for (int j = 0; j < kLeaf; ++j) x[j] = (j < cols) ? B[(long long)j * ldb + row] : 0.f;
+    for (int i = 0; i < kLeaf; ++i) x[i] = (i == t) ? 1.f : 0.f;
 #pragma unroll
     for (int k = 0; k < kLeaf; ++k) {
-        if (k < cols) {
-            x[k] *= rd[k];
+        if (k < nb) {
+            if (!unit) x[k] = x[k] / Ls[k][k];
 #pragma unroll
-            for (int j = k + 1; j < kLeaf; ++j) x[j] = fmaf(-Ls[k][j], x[k], x[j]);
+            for (int i = k + 1; i < kLeaf; ++i) x[i] = fmaf(-Ls[i][k], x[k], x[i]);
         }
     }
+    float* o = out + (long long)blockIdx.x * kLeaf * kLeaf + (long long)t * kLeaf;
 #pragma unroll
-    for (int j = 0; j < kLeaf; ++j)
-        if (j < cols) B[(long long)j * ldb + row] = x[j];
+    for (int i = 0; i < kLeaf; ++i) o[i] = x[i];
 }
 
-// B(rows x cols) <- L^{-1} B, L unit lower (rows <= 64): one thread per
-// column; the CTA's 128 columns are staged through shared memory so global
-// traffic stays coalesced down each column.
-constexpr int kLluCols = 128;
-__global__ void __launch_bounds__(kLluCols) trsm_llu_kernel(int rows, int cols,
-                                                            const float* __restrict__ L,
-                                                            long long ldl, float* B,
-                                                            long long ldb)
+// B(rows x cols) <- inv * B for rows <= 64 (inv = L^{-1} of the leaf block):
+// CTA = 64 x 64 tile of B, thread = 4 x 4 outputs, in place.
+__global__ void __launch_bounds__(256) llu_apply_kernel(int rows, int cols,
+                                                        const float* __restrict__ inv, float* B,
+                                                        long long ldb)
 {
-    extern __shared__ float sm[];
-    float* Ls = sm;                       // [kLeaf][kLeaf]  Ls[c*64 + r] = L(r, c)
-    float* Bs = sm + kLeaf * kLeaf;       // [kLeaf][kLluCols + 1]
-    constexpr int BST = kLluCols + 1;
+    __shared__ __align__(16) float Is[kLeaf][kLeaf];  // Is[k][r] = inv(r, k)
+    __shared__ __align__(16) float Bs[kLeaf][kLeaf];  // Bs[k][c] = B(k, c0 + c)
     const int tid = threadIdx.x;
-    const long long c0 = (long long)blockIdx.x * kLluCols;
-    for (int idx = tid; idx < kLeaf * kLeaf; idx += blockDim.x) {
-        const int c = idx / kLeaf, r = idx - c * kLeaf;
-        Ls[idx] = (r < rows && c < rows && r > c) ? L[(long long)c * ldl + r] : 0.f;
-    }
-    for (int idx = tid; idx < rows * kLluCols; idx += blockDim.x) {
-        const int c = idx / rows, r = idx - c * rows;
-        const long long gc = c0 + c;
-        Bs[r * BST + c] = (gc < cols) ? B[gc * ldb + r] : 0.f;
+    const long long c0 = (long long)blockIdx.x * kLeaf;
+    for (int idx = tid; idx < kLeaf * kLeaf; idx += 256) {
+        const int k = idx >> 6, r = idx & 63;
+        Is[k][r] = inv[idx];
+        const int c = idx >> 6, kk = idx & 63;
+        Bs[kk][c] = (kk < rows && c0 + c < cols) ? B[(c0 + c) * ldb + kk] : 0.f;
     }
     __syncthreads();
-    float x[kLeaf];
+    const int ty = tid >> 4, tx = tid & 15;
+    float acc[4][4] = {};
+#pragma unroll 16
+    for (int k = 0; k < kLeaf; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(&Is[k][ty * 4]);
+        const float4 b = *reinterpret_cast<const float4*>(&Bs[k][tx * 4]);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+        const float bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-    for (int r = 0; r < kLeaf; ++r) x[r] = (r < rows) ? Bs[r * BST + tid] : 0.f;
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int p = 0; p < kLeaf; ++p) {
-        if (p < rows) {
+            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
 #pragma unroll
-            for (int i = p + 1; i < kLeaf; ++i) x[i] = fmaf(-Ls[p * kLeaf + i], x[p], x[i]);
+    for (int j = 0; j < 4; ++j) {
+        const long long c = c0 + tx * 4 + j;
+        if (c >= cols) continue;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = ty * 4 + i;
+            if (r < rows) B[c * ldb + r] = acc[i][j];
         }
-    }
-#pragma unroll
-    for (int r = 0; r < kLeaf; ++r)
-        if (r < rows) Bs[r * BST + tid] = x[r];
-    __syncthreads();
-    for (int idx = tid; idx < rows * kLluCols; idx += blockDim.x) {
-        const int c = idx / rows, r = idx - c * rows;
-        const long long gc = c0 + c;
-        if (gc < cols) B[gc * ldb + r] = Bs[r * BST + c];
     }
 }
 
-constexpr size_t kLluSmem = (size_t)(kLeaf * kLeaf + kLeaf * (kLluCols + 1)) * sizeof(float);
+// B(rows x cols) <- B * inv^T for cols <= 64 (inv = L^{-1} of the leaf
+// block): CTA = 128 x 64 tile of B, thread = 8 rows x 4 columns, in place.
+__global__ void __launch_bounds__(256) rlt_apply_kernel(int rows, int cols,
+                                                        const float* __restrict__ inv, float* B,
+                                                        long long ldb)
+{
+    __shared__ __align__(16) float Bs[kLeaf][128];   // Bs[k][r] = B(r0 + r, k)
+    __shared__ __align__(16) float Is[kLeaf][kLeaf];  // Is[k][c] = inv(c, k)
+    const int tid = threadIdx.x;
+    const long long r0 = (long long)blockIdx.x * 128;
+    for (int idx = tid; idx < kLeaf * kLeaf; idx += 256) Is[idx >> 6][idx & 63] = inv[idx];
+    for (int idx = tid; idx < kLeaf * 128; idx += 256) {
+        const int k = idx >> 7, r = idx & 127;
+        Bs[k][r] = (k < cols && r0 + r < rows) ? B[(long long)k * ldb + r0 + r] : 0.f;
+    }
+    __syncthreads();
+    const int ty = tid >> 4, tx = tid & 15;
+    float acc[8][4] = {};
+#pragma unroll 8
+    for (int k = 0; k < kLeaf; ++k) {
+        const float4 a0 = *reinterpret_cast<const float4*>(&Bs[k][ty * 8]);
+        const float4 a1 = *reinterpret_cast<const float4*>(&Bs[k][ty * 8 + 4]);
+        const float4 b = *reinterpret_cast<const float4*>(&Is[k][tx * 4]);
+        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+        const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int c = tx * 4 + j;
+        if (c >= cols) continue;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const long long r = r0 + ty * 8 + i;
+            if (r < rows) B[(long long)c * ldb + r] = acc[i][j];
+        }
+    }
+}
 
 }  // namespace
 
@@ -162,34 +213,38 @@ hdbf_status potf2_small(hdbf_context* ctx, int n, float* A, long long lda, int* 
     return last_cuda(ctx);
 }
 
-hdbf_status trsm_rlt_small(hdbf_context* ctx, int rows, int cols, const float* L,
-                           long long ldl, float* B, long long ldb)
+hdbf_status tri_inv64(hdbf_context* ctx, int n, const float* L, long long ldl, bool unit,
+                      float* out)
 {
-    if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
-    if (cols > kLeaf) return HDBF_STATUS_INVALID_VALUE;
-    const long long grid = ((long long)rows + kRltThreads - 1) / kRltThreads;
-    ProfScope prof(ctx, kClsTrsmR, (double)rows * cols * cols, 8.0 * rows * cols);
-    trsm_rlt_kernel<<<(unsigned)grid, kRltThreads, 0, ctx->stream>>>(rows, cols, L, ldl, B,
-                                                                      ldb);
+    if (n <= 0) return HDBF_STATUS_SUCCESS;
+    const int blocks = (n + kLeaf - 1) / kLeaf;
+    ProfScope prof(ctx, kClsTrsmInv, (double)blocks * kLeaf * kLeaf * kLeaf / 3.0,
+                   8.0 * blocks * kLeaf * kLeaf);
+    tri_inv64_kernel<<<blocks, kLeaf, 0, ctx->stream>>>(n, L, ldl, unit ? 1 : 0, out);
     ctx->launches++;
     return last_cuda(ctx);
 }
 
-hdbf_status trsm_llu_small(hdbf_context* ctx, int rows, int cols, const float* L,
-                           long long ldl, float* B, long long ldb)
+hdbf_status llu_apply(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
+                      long long ldb)
 {
     if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
     if (rows > kLeaf) return HDBF_STATUS_INVALID_VALUE;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(trsm_llu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kLluSmem);
-        configured = true;
-    }
-    const long long grid = ((long long)cols + kLluCols - 1) / kLluCols;
-    ProfScope prof(ctx, kClsTrsmL, (double)cols * rows * rows, 8.0 * rows * cols);
-    trsm_llu_kernel<<<(unsigned)grid, kLluCols, kLluSmem, ctx->stream>>>(rows, cols, L, ldl,
-                                                                         B, ldb);
+    const long long grid = ((long long)cols + kLeaf - 1) / kLeaf;
+    ProfScope prof(ctx, kClsTrsmL, 2.0 * kLeaf * kLeaf * (double)cols, 8.0 * rows * cols);
+    llu_apply_kernel<<<(unsigned)grid, 256, 0, ctx->stream>>>(rows, cols, inv, B, ldb);
+    ctx->launches++;
+    return last_cuda(ctx);
+}
+
+hdbf_status rlt_apply(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
+                      long long ldb)
+{
+    if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
+    if (cols > kLeaf) return HDBF_STATUS_INVALID_VALUE;
+    const long long grid = ((long long)rows + 127) / 128;
+    ProfScope prof(ctx, kClsTrsmR, 2.0 * kLeaf * kLeaf * (double)rows, 8.0 * rows * cols);
+    rlt_apply_kernel<<<(unsigned)grid, 256, 0, ctx->stream>>>(rows, cols, inv, B, ldb);
     ctx->launches++;
     return last_cuda(ctx);
 }

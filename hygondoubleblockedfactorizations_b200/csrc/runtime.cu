@@ -1,4 +1,5 @@
 // Handle, stream pool, workspace arena and status plumbing (host C++).
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -14,21 +15,25 @@ hdbf_status last_cuda(hdbf_context* ctx)
     return e == cudaSuccess ? HDBF_STATUS_SUCCESS : HDBF_STATUS_CUDA_ERROR;
 }
 
+static int fitting_order(size_t bytes);
+
 void* workspace(hdbf_context* ctx, size_t bytes, hdbf_status* st)
 {
     *st = HDBF_STATUS_SUCCESS;
-    if (bytes <= ctx->ws_bytes) return ctx->ws;
+    if (bytes <= ctx->ws_bytes && ctx->ws) return ctx->ws;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(ctx->stream, &cs) == cudaSuccess &&
         cs != cudaStreamCaptureStatusNone) {
         *st = HDBF_STATUS_WORKSPACE_TOO_SMALL;
         return nullptr;
     }
+    graph_cache_clear(ctx);  // cached graphs point into the old arena
     if (ctx->ws) {
         cudaStreamSynchronize(ctx->stream);
         cudaFree(ctx->ws);
         ctx->ws = nullptr;
         ctx->ws_bytes = 0;
+        ctx->ws_n = 0;
     }
     size_t want = align_up(bytes, size_t(1) << 20);
     if (cudaMalloc(&ctx->ws, want) != cudaSuccess) {
@@ -38,36 +43,220 @@ void* workspace(hdbf_context* ctx, size_t bytes, hdbf_status* st)
         return nullptr;
     }
     ctx->ws_bytes = want;
+    ctx->ws_n = fitting_order(want);
+    // The panel kernel's exchange slots must never hold a stale sequence
+    // number that matches a live one: clear them on every (re)allocation.
+    cudaMemset(ctx->ws, 0, getf2_coop_scratch_bytes() < want ? getf2_coop_scratch_bytes() : want);
+    cudaDeviceSynchronize();
     return ctx->ws;
 }
 
-static cudaEvent_t pool_event(hdbf_context* ctx)
+WsLayout ws_layout(int n)
 {
-    if (ctx->ev_used == ctx->ev_pool.size()) {
-        cudaEvent_t e;
-        if (cudaEventCreate(&e) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        ctx->ev_pool.push_back(e);
-    }
-    return ctx->ev_pool[ctx->ev_used++];
+    if (n < 64) n = 64;
+    WsLayout L;
+    size_t off = 0;
+    L.coop = off;
+    off += getf2_coop_scratch_bytes();
+    L.inv = off;
+    off += align_up((size_t)n * 64 * sizeof(float), 256);
+    L.src = off;
+    off += align_up((size_t)n * sizeof(int), 256);
+    L.tgt = off;
+    off += align_up((size_t)n * sizeof(int), 256);
+    L.gperm = off;
+    off += align_up((size_t)n * sizeof(int), 256);
+    L.temp = off;
+    off += align_up((size_t)64 * n * sizeof(float), 256);
+    L.total = off;
+    return L;
 }
 
-ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes) : ctx_(ctx)
+static int fitting_order(size_t bytes)
+{
+    if (ws_layout(64).total > bytes) return 0;
+    int lo = 64, hi = 1 << 24;
+    while (lo < hi) {
+        const int mid = lo + (hi - lo + 1) / 2;
+        if (ws_layout(mid).total <= bytes) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+hdbf_status ensure_ws(hdbf_context* ctx, int n)
+{
+    if (n <= ctx->ws_n && ctx->ws) return HDBF_STATUS_SUCCESS;
+    const int want = n > ctx->ws_n ? n : ctx->ws_n;
+    hdbf_status st;
+    workspace(ctx, ws_layout(want).total, &st);
+    return st;
+}
+
+float* ws_coop(hdbf_context* ctx)
+{
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).coop);
+}
+float* ws_inv(hdbf_context* ctx)
+{
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).inv);
+}
+int* ws_src(hdbf_context* ctx)
+{
+    return reinterpret_cast<int*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).src);
+}
+int* ws_tgt(hdbf_context* ctx)
+{
+    return reinterpret_cast<int*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).tgt);
+}
+int* ws_gperm(hdbf_context* ctx)
+{
+    return reinterpret_cast<int*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).gperm);
+}
+float* ws_temp(hdbf_context* ctx)
+{
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).temp);
+}
+
+ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes, int m, int n,
+                     int k)
+    : ctx_(ctx)
 {
     if (!ctx || !ctx->profiling) return;
-    cudaEvent_t a = pool_event(ctx), b = pool_event(ctx);
-    if (!a || !b) return;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        cudaGetLastError();
+        if (a) cudaEventDestroy(a);
+        return;
+    }
     cudaEventRecord(a, ctx->stream);
     idx_ = static_cast<int>(ctx->prof.size());
-    ctx->prof.push_back(ProfRec{cls, a, b, flops, bytes});
+    ctx->prof.push_back(ProfRec{cls, a, b, flops, bytes, m, n, k});
 }
 
 ProfScope::~ProfScope()
 {
     if (idx_ < 0) return;
     cudaEventRecord(ctx_->prof[idx_].b, ctx_->stream);
+}
+
+static void destroy_records(std::vector<ProfRec>& v)
+{
+    for (ProfRec& r : v) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    v.clear();
+}
+
+// ------------------------------------------------------------------ graphs
+constexpr size_t kMaxGraphs = 12;
+
+void graph_cache_clear(hdbf_context* ctx)
+{
+    for (GraphEntry& e : ctx->graphs) {
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+        destroy_records(e.prof);
+    }
+    ctx->graphs.clear();
+    ctx->prof_graph_ids.clear();
+}
+
+bool graph_can_capture(hdbf_context* ctx)
+{
+    if (!ctx->use_graphs || ctx->capturing) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return cs == cudaStreamCaptureStatusNone;  // the caller is not capturing us itself
+}
+
+GraphEntry* graph_find(hdbf_context* ctx, const std::vector<long long>& key)
+{
+    for (GraphEntry& e : ctx->graphs)
+        if (e.key == key) return &e;
+    return nullptr;
+}
+
+hdbf_status graph_capture_begin(hdbf_context* ctx, cudaStream_t* saved)
+{
+    if (!ctx->cap_stream &&
+        cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    if (cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    *saved = ctx->stream;
+    ctx->stream = ctx->cap_stream;
+    ctx->capturing = true;
+    return HDBF_STATUS_SUCCESS;
+}
+
+hdbf_status graph_capture_end(hdbf_context* ctx, cudaStream_t saved, hdbf_status body_status,
+                              const std::vector<long long>& key, size_t prof_mark,
+                              unsigned long long launches_before)
+{
+    const unsigned long long kernels = ctx->launches - launches_before;
+    ctx->launches = launches_before;  // counted when the graph actually runs
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(ctx->cap_stream, &graph);
+    ctx->stream = saved;
+    ctx->capturing = false;
+    std::vector<ProfRec> recs(ctx->prof.begin() + prof_mark, ctx->prof.end());
+    ctx->prof.resize(prof_mark);
+    if (ce != cudaSuccess || !graph) {
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        destroy_records(recs);
+        ctx->use_graphs = false;  // this work cannot be captured here: stay eager
+        return HDBF_STATUS_NOT_SUPPORTED;
+    }
+    if (body_status != HDBF_STATUS_SUCCESS) {
+        cudaGraphDestroy(graph);
+        destroy_records(recs);
+        return body_status;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        cudaGetLastError();
+        destroy_records(recs);
+        ctx->use_graphs = false;
+        return HDBF_STATUS_NOT_SUPPORTED;
+    }
+    if (ctx->graphs.size() >= kMaxGraphs) {  // evict the least recently used
+        size_t lru = 0;
+        for (size_t i = 1; i < ctx->graphs.size(); ++i)
+            if (ctx->graphs[i].last_use < ctx->graphs[lru].last_use) lru = i;
+        cudaGraphExecDestroy(ctx->graphs[lru].exec);
+        destroy_records(ctx->graphs[lru].prof);
+        ctx->graphs.erase(ctx->graphs.begin() + lru);
+    }
+    GraphEntry e;
+    e.key = key;
+    e.exec = exec;
+    e.prof = std::move(recs);
+    e.id = ++ctx->graph_clock;
+    e.kernels = kernels;
+    ctx->graphs.push_back(std::move(e));
+    return graph_launch(ctx, &ctx->graphs.back());
+}
+
+hdbf_status graph_launch(hdbf_context* ctx, GraphEntry* e)
+{
+    e->last_use = ++ctx->graph_clock;
+    if (ctx->profiling && !e->prof.empty()) ctx->prof_graph_ids.push_back(e->id);
+    if (cudaGraphLaunch(e->exec, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    ctx->launches += e->kernels;
+    return HDBF_STATUS_SUCCESS;
 }
 
 }  // namespace hdbf
@@ -97,6 +286,9 @@ hdbf_status hdbf_create(hdbf_handle* handle)
         return HDBF_STATUS_ALLOC_FAILED;
     }
     cudaMemset(ctx->dev_small, 0, kSmallInts * sizeof(int));
+    configure_getrf_kernels(ctx);
+    const int one = 1;  // exchange epoch starts at 1: zeroed slots never match
+    cudaMemcpy(ctx->dev_small + kSmallEpoch, &one, sizeof(int), cudaMemcpyHostToDevice);
     cudaDeviceSynchronize();
     *handle = ctx;
     return HDBF_STATUS_SUCCESS;
@@ -106,7 +298,9 @@ hdbf_status hdbf_destroy(hdbf_handle h)
 {
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
     cudaStreamSynchronize(h->stream);
-    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    graph_cache_clear(h);
+    destroy_records(h->prof);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->ws) cudaFree(h->ws);
     if (h->dev_small) cudaFree(h->dev_small);
     delete h;
@@ -149,17 +343,7 @@ const char* hdbf_status_string(hdbf_status s)
     return "unknown status";
 }
 
-size_t hdbf_workspace_bytes_for(int n)
-{
-    if (n < 1) n = 1;
-    // coop panel scratch + compose moves (src, tgt, gperm: 3 n ints) +
-    // a column-tiled swap buffer (64 columns x n floats) + slack.
-    size_t b = getf2_coop_scratch_bytes();
-    b += 3 * align_up(size_t(n) * sizeof(int), 256);
-    b += align_up(size_t(64) * size_t(n) * sizeof(float), 256);
-    b += size_t(1) << 20;
-    return b;
-}
+size_t hdbf_workspace_bytes_for(int n) { return ws_layout(n < 1 ? 1 : n).total; }
 
 hdbf_status hdbf_reserve_workspace(hdbf_handle h, size_t bytes)
 {
@@ -183,8 +367,13 @@ hdbf_status hdbf_check_device_errors(hdbf_handle h)
         return HDBF_STATUS_CUDA_ERROR;
     }
     if (err != 0) {
-        // Clear the error word and re-arm the grid barrier for later launches.
+        // Clear the error word and the exchange counters, and advance the
+        // epoch past every sequence number a timed-out launch may have left.
+        unsigned epoch = 0;
+        cudaMemcpy(&epoch, h->dev_small + kSmallEpoch, sizeof(int), cudaMemcpyDeviceToHost);
         cudaMemset(h->dev_small, 0, kSmallInts * sizeof(int));
+        epoch += 2;
+        cudaMemcpy(h->dev_small + kSmallEpoch, &epoch, sizeof(int), cudaMemcpyHostToDevice);
         cudaDeviceSynchronize();
         return err == kErrTimeout ? HDBF_STATUS_TIMEOUT : HDBF_STATUS_INVALID_VALUE;
     }
@@ -239,8 +428,8 @@ unsigned long long hdbf_launch_count(hdbf_handle h) { return h ? h->launches : 0
 hdbf_status hdbf_profile_begin(hdbf_handle h)
 {
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
-    h->prof.clear();
-    h->ev_used = 0;
+    destroy_records(h->prof);
+    h->prof_graph_ids.clear();
     h->profiling = true;
     return HDBF_STATUS_SUCCESS;
 }
@@ -260,32 +449,61 @@ hdbf_status hdbf_profile_end(hdbf_handle h, int max_classes, double* ms, double*
         if (bytes) bytes[c] = 0.0;
         if (launches) launches[c] = 0;
     }
-    for (const ProfRec& r : h->prof) {
-        if (r.cls < 0 || r.cls >= max_classes) continue;
+    // HDBF_PROFILE_CSV=<path>: also append one line per launch (class, ms,
+    // flops, bytes, m, n, k) for offline analysis.
+    const char* csv_path = std::getenv("HDBF_PROFILE_CSV");
+    FILE* csv = csv_path ? std::fopen(csv_path, "a") : nullptr;
+    auto add = [&](const ProfRec& r) {
+        if (r.cls < 0 || r.cls >= max_classes) return;
         float t = 0.f;
         if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) {
             cudaGetLastError();
-            continue;
+            return;
         }
+        if (csv)
+            std::fprintf(csv, "%s,%.6f,%.6g,%.6g,%d,%d,%d\n", hdbf_profile_class_name(r.cls), t,
+                         r.flops, r.bytes, r.m, r.n, r.k);
         if (ms) ms[r.cls] += t;
         if (flops) flops[r.cls] += r.flops;
         if (bytes) bytes[r.cls] += r.bytes;
         if (launches) launches[r.cls] += 1;
+    };
+    for (const ProfRec& r : h->prof) add(r);
+    // Graphs replayed while profiling: their event nodes hold the timings of
+    // the latest replay (each graph counted once).
+    std::vector<unsigned long long> seen;
+    for (unsigned long long id : h->prof_graph_ids) {
+        bool dup = false;
+        for (unsigned long long s2 : seen) dup = dup || s2 == id;
+        if (dup) continue;
+        seen.push_back(id);
+        for (const GraphEntry& e : h->graphs)
+            if (e.id == id)
+                for (const ProfRec& r : e.prof) add(r);
     }
-    h->prof.clear();
-    h->ev_used = 0;
+    if (csv) std::fclose(csv);
+    destroy_records(h->prof);
+    h->prof_graph_ids.clear();
     return HDBF_STATUS_SUCCESS;
 }
 
 const char* hdbf_profile_class_name(int cls)
 {
     static const char* names[kNumClasses] = {"sgemm_sub_kernel", "potf2_kernel",
-                                             "trsm_rlt_kernel", "trsm_llu_kernel",
+                                             "rlt_apply_kernel", "llu_apply_kernel",
                                              "getf2_coop_kernel", "compose_swaps_kernel",
-                                             "apply_moves", "other"};
+                                             "apply_moves", "tri_inv64_kernel", "other"};
     return (cls >= 0 && cls < kNumClasses) ? names[cls] : "unknown";
 }
 
 int hdbf_profile_num_classes(void) { return kNumClasses; }
+
+hdbf_status hdbf_set_graph_mode(hdbf_handle h, int enabled)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    h->use_graphs = enabled != 0;
+    if (!h->use_graphs) graph_cache_clear(h);
+    return HDBF_STATUS_SUCCESS;
+}
 
 }  // extern "C"

@@ -192,7 +192,8 @@ hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N,
         const double d = (double)(M < N ? M : N);
         flops = 2.0 * (double)K * (d * (double)M - d * (d - 1.0) / 2.0);
     }
-    ProfScope prof(ctx, kClsGemm, flops, 4.0 * ((double)M * K + (double)N * K + 2.0 * M * N));
+    ProfScope prof(ctx, kClsGemm, flops, 4.0 * ((double)M * K + (double)N * K + 2.0 * M * N), M,
+                   N, K);
 #define HDBF_SUB(NNv, VECv, TRIv) launch_sub<NNv, VECv, TRIv>(s, M, N, K, A, lda, B, ldb, C, ldc)
     if (nn) {
         if (vec) { if (lower_only) HDBF_SUB(true, true, true); else HDBF_SUB(true, true, false); }

@@ -78,6 +78,13 @@ hdbf_status hdbf_fill_uniform(hdbf_handle handle, float* x, size_t count,
  * (a host-side counter; used to report gpu_launches). */
 unsigned long long hdbf_launch_count(hdbf_handle handle);
 
+/* Whole-factorization CUDA graphs (default on).  When enabled, the first
+ * call of a factorization entry point with a given argument tuple records its
+ * kernel chain as a CUDA graph; later calls with identical arguments replay it
+ * on the handle's stream.  Calls made while the caller is itself capturing the
+ * stream are recorded into the caller's graph instead. */
+hdbf_status hdbf_set_graph_mode(hdbf_handle handle, int enabled);
+
 /* Per-launch event profiling of this library's kernels on the handle's
  * stream.  Between begin and end every launch is bracketed by CUDA events;
  * end synchronises the stream and returns, per kernel class (see

@@ -209,6 +209,43 @@ def double_blocked_getrf(A2d: np.ndarray, outer_nb: int, inner_nb: int):
     return A, ipiv, info
 
 
+def pivot_divergence(A2d: np.ndarray, ipiv_a, ipiv_b):
+    """First index where two LAPACK pivot sequences differ, and how close the
+    pivot choice was there.
+
+    Returns (None, None) when identical.  Otherwise (j, rel_gap): the common
+    prefix of pivots is applied to A, the Schur complement column j is formed
+    in FP64 (S = A22 - A21 A11^{-1} A12, column j), and rel_gap = (|s|_1st -
+    |s|_2nd) / |s|_1st over the candidate rows.  A rel_gap at the level of FP32
+    rounding (<~ 1e-4) marks a near-tie, where any FP32 implementation may
+    legitimately choose either row.
+    """
+    a = np.asarray(ipiv_a).astype(np.int64)
+    b = np.asarray(ipiv_b).astype(np.int64)
+    diff = np.nonzero(a != b)[0]
+    if diff.size == 0:
+        return None, None
+    j = int(diff[0])
+    n = A2d.shape[0]
+    M = np.array(A2d, dtype=np.float64)
+    perm = np.arange(n)
+    for r in range(j):
+        p = a[r] - 1
+        perm[r], perm[p] = perm[p], perm[r]
+    M = M[perm, :]
+    if j > 0:
+        x = np.linalg.solve(M[:j, :j], M[:j, j])
+        col = M[j:, j] - M[j:, :j] @ x
+    else:
+        col = M[:, 0].copy()
+    mag = np.sort(np.abs(col))[::-1]
+    gap = (mag[0] - mag[1]) / mag[0] if mag.size > 1 and mag[0] > 0 else 0.0
+    return j, float(gap)
+
+
+NEAR_TIE = 1e-4
+
+
 def parse_seed(text):
     seed = ctypes.c_uint(19)
     ok = lib().oracle_parse_seed(None if text is None else text.encode(), ctypes.byref(seed))

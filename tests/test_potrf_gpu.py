@@ -133,3 +133,28 @@ def test_device_generator_matches_oracle(hd, handle, torch_cuda):
     torch_cuda.cuda.synchronize()
     assert st == 0
     np.testing.assert_array_equal(x.cpu().numpy(), oracle.uniform_pm1(100003, 0, offset=17))
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_graph_replay_matches_eager(hd, handle, torch_cuda, graphs):
+    """The second call with identical arguments replays the recorded CUDA graph;
+    results must equal the first (captured) call and the eager path bit for bit."""
+    n = 1536
+    A = oracle.spd_gram(n, 4)
+    handle.set_graphs(graphs)
+    d0 = dev(torch_cuda, A)
+    d = d0.clone()
+    info = info_tensor(torch_cuda)
+    outs = []
+    for _ in range(3):
+        d.copy_(d0)
+        hd.call("double_blocked_potrf_kblocked_syrk", handle.ptr, ptr(d), n, n, 512, 128, 256,
+                ptr(info))
+        torch_cuda.cuda.synchronize()
+        handle.check()
+        assert int(info.item()) == 0
+        outs.append(d.cpu().numpy().copy())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[1], outs[2])
+    L = outs[2].reshape(n, n).T
+    assert potrf_check(np.tril(L), A) <= BOUND
