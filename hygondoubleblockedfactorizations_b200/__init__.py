@@ -75,6 +75,8 @@ _PROTOS = {
     "iterative_trsm_right_looking": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
     "gemm_nt_update": (None, [P, c_int, c_int, c_int, P, c_int, P, c_int, P, c_int]),
     "gemm_nt_update_m_tiled": (None, [P, c_int, c_int, c_int, P, c_int, P, c_int, P, c_int, c_int]),
+    "launch_mixed_gemm": (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_float, P, c_int, P,
+                                 c_int, c_float, P, c_int]),
     # kernels
     "launch_add_damping": (None, [P, c_int, c_int, c_float, P]),
     "launch_add_damping_double": (None, [P, c_int, c_int, c_double, P]),

@@ -238,27 +238,21 @@ __global__ void __launch_bounds__(kComposeThreads)
 compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m, int* src,
                      int* tgt, int* count, int* gperm, int use_smem, int* info, int* err)
 {
+    // Shared layout (use_smem): perm[m] then the k pivots; otherwise perm
+    // lives in global scratch and the pivots are re-read from global memory.
     extern __shared__ int sperm[];
     __shared__ int warp_tot[kComposeThreads / 32];
     __shared__ int s_base, s_bad, s_chunk;
     int* perm = use_smem ? sperm : gperm;
+    int* piv = use_smem ? sperm + m : nullptr;
     const int tid = threadIdx.x;
-    for (int q = tid; q < m; q += kComposeThreads) perm[q] = q;
-    if (tid == 0) s_bad = 0;
+    if (tid == 0) { s_bad = 0; s_base = 0; }
     __syncthreads();
-    if (tid == 0) {
-        int bad = 0;
-        for (int i = 0; i < k; ++i) {
-            const int b = ipiv[i] - 1 - ipiv_minus;
-            if (b < i || b >= m) { bad = 1; break; }
-            if (b != i) {
-                const int t = perm[i];
-                perm[i] = perm[b];
-                perm[b] = t;
-            }
-        }
-        s_bad = bad;
-        s_base = 0;
+    for (int q = tid; q < m; q += kComposeThreads) perm[q] = q;
+    for (int i = tid; i < k; i += kComposeThreads) {
+        const int b = ipiv[i] - 1 - ipiv_minus;
+        if (b < i || b >= m) s_bad = 1;
+        if (piv) piv[i] = b;
     }
     __syncthreads();
     if (s_bad) {
@@ -269,12 +263,25 @@ compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m,
         }
         return;
     }
-    // Ordered compaction of the rows whose content changed.
+    // The swap sequence itself is inherently ordered: one thread replays it.
+    if (tid == 0) {
+        for (int i = 0; i < k; ++i) {
+            const int b = piv ? piv[i] : ipiv[i] - 1 - ipiv_minus;
+            if (b != i) {
+                const int t = perm[i];
+                perm[i] = perm[b];
+                perm[b] = t;
+            }
+        }
+    }
+    __syncthreads();
+    // Moves: rows [0, k) in order (ordered block scan), then the distinct
+    // pivot rows >= k (each claimed once by flipping its entry negative).
     const int lane = tid & 31, warp = tid >> 5;
-    for (int q0 = 0; q0 < m; q0 += kComposeThreads) {
+    for (int q0 = 0; q0 < k; q0 += kComposeThreads) {
         const int q = q0 + tid;
-        const int s = (q < m) ? perm[q] : q;
-        const bool moved = (q < m) && (s != q);
+        const int s = (q < k) ? perm[q] : q;
+        const bool moved = (q < k) && (s != q);
         const unsigned ball = __ballot_sync(0xffffffffu, moved);
         const int within = __popc(ball & ((1u << lane) - 1u));
         if (lane == 0) warp_tot[warp] = __popc(ball);
@@ -298,6 +305,17 @@ compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m,
         if (tid == 0) s_base += s_chunk;
         __syncthreads();
     }
+    for (int i = tid; i < k; i += kComposeThreads) {
+        const int b = piv ? piv[i] : ipiv[i] - 1 - ipiv_minus;
+        if (b < k) continue;
+        const int s = atomicExch(&perm[b], -1);  // claim position b once
+        if (s >= 0 && s != b) {
+            const int pos = atomicAdd(&s_base, 1);
+            src[pos] = s;
+            tgt[pos] = b;
+        }
+    }
+    __syncthreads();
     if (tid == 0) *count = s_base;
 }
 
@@ -418,7 +436,7 @@ hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_mi
                           int* src, int* tgt, int* count, int* gperm, int* info)
 {
     if (k <= 0 || m <= 0) return HDBF_STATUS_SUCCESS;
-    const size_t smem = (size_t)m * sizeof(int);
+    const size_t smem = ((size_t)m + (size_t)k) * sizeof(int);
     const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
     const int use_smem = smem <= cap ? 1 : 0;
     if (!use_smem && !gperm) return HDBF_STATUS_INVALID_VALUE;

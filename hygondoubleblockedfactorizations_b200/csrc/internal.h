@@ -19,8 +19,11 @@ enum KernelClass {
     kClsCompose = 5,  // compose_swaps_kernel
     kClsMoves = 6,    // apply_moves kernels
     kClsTrsmInv = 7,  // tri_inv64_kernel
-    kClsOther = 8,
-    kNumClasses = 9
+    kClsTcGemm = 8,   // tc_gemm_sub_kernel (tcgen05 mixed-precision updates)
+    kClsConvert = 9,  // FP32 -> 16-bit shadow conversions
+    kClsIr = 10,      // FP64 residual / update / norm kernels
+    kClsOther = 11,
+    kNumClasses = 12
 };
 struct ProfRec {
     int cls;
@@ -50,6 +53,10 @@ struct hdbf_context {
     int ws_n = 0;  // largest order whose layout fits in ws_bytes
     // Small always-present device block: [0] error word, [1..] barrier words.
     int* dev_small = nullptr;
+    // Second arena for the mixed-precision path (16-bit shadows, FP64 IR
+    // vectors); grown on demand outside stream capture.
+    void* mix = nullptr;
+    size_t mix_bytes = 0;
     hdbf_status last_status = HDBF_STATUS_SUCCESS;
     unsigned long long launches = 0;
     // Optional per-launch event profiling.
@@ -102,6 +109,9 @@ private:
 // Make sure the workspace holds at least `bytes`; returns nullptr and sets
 // *st on failure.  Growing frees the old buffer (device-synchronising).
 void* workspace(hdbf_context* ctx, size_t bytes, hdbf_status* st);
+
+// Mixed-path arena of at least `bytes` (same growth rules as the workspace).
+void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st);
 
 // Workspace layout for problems of order <= n (byte offsets):
 //   coop  panel-kernel exchange slots (fixed size, offset 0)
@@ -163,6 +173,30 @@ hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_mi
 hdbf_status apply_moves(hdbf_context* ctx, float* A, long long lda, int ncols,
                         const int* src, const int* tgt, const int* count, int max_moves,
                         float* temp, long long temp_cols);
+
+// ------------------------------------------------ tensor-core (tcgen05) path
+// A K-major 16-bit operand: row r, element k at base[(row0 + r) * ld + k0 + k].
+struct TcOperand {
+    const void* base = nullptr;
+    long long ld = 0;  // elements; multiple of 8
+    int row0 = 0;
+    int k0 = 0;        // multiple of 8
+};
+constexpr int kFmtF16 = 0;   // IEEE binary16
+constexpr int kFmtBF16 = 1;  // bfloat16
+// C(M x N, FP32 column-major) -= scale * A * B^T on the tensor cores.
+hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
+                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only);
+void configure_tc_kernels(hdbf_context* ctx);
+// dst(r, k) = round16(s * src(r, k)) for an rows x cols FP32 column-major block
+// into a K-major (row-major, ldd elements) 16-bit block; `hi_lo` additionally
+// writes the rounding residual round16(s*src - hi) into lo (may be null).
+hdbf_status convert_transpose16(hdbf_context* ctx, int fmt, int rows, int cols, const float* src,
+                                long long lds, void* hi, void* lo, long long ldd, float s);
+// dst[c * ldd + r] = round16(s * src[c * lds + r]): same layout (column-major
+// FP32 -> "column = K-major row" 16-bit), with optional residual.
+hdbf_status convert_direct16(hdbf_context* ctx, int fmt, int rows, int cols, const float* src,
+                             long long lds, void* hi, void* lo, long long ldd, float s);
 
 // Auxiliary kernels.
 hdbf_status fill_uniform(hdbf_context* ctx, float* x, size_t count, uint64_t seed,

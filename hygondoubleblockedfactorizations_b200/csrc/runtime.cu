@@ -51,6 +51,34 @@ void* workspace(hdbf_context* ctx, size_t bytes, hdbf_status* st)
     return ctx->ws;
 }
 
+void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st)
+{
+    *st = HDBF_STATUS_SUCCESS;
+    if (bytes <= ctx->mix_bytes && ctx->mix) return ctx->mix;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &cs) == cudaSuccess &&
+        cs != cudaStreamCaptureStatusNone) {
+        *st = HDBF_STATUS_WORKSPACE_TOO_SMALL;
+        return nullptr;
+    }
+    graph_cache_clear(ctx);  // cached graphs point into the old arena
+    if (ctx->mix) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->mix);
+        ctx->mix = nullptr;
+        ctx->mix_bytes = 0;
+    }
+    const size_t want = align_up(bytes, size_t(1) << 20);
+    if (cudaMalloc(&ctx->mix, want) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->mix = nullptr;
+        *st = HDBF_STATUS_ALLOC_FAILED;
+        return nullptr;
+    }
+    ctx->mix_bytes = want;
+    return ctx->mix;
+}
+
 WsLayout ws_layout(int n)
 {
     if (n < 64) n = 64;
@@ -128,7 +156,9 @@ ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes, int
         if (a) cudaEventDestroy(a);
         return;
     }
-    cudaEventRecord(a, ctx->stream);
+    // Under capture the record must become a real event node of the graph
+    // (a plain record would only express a dependency).
+    cudaEventRecordWithFlags(a, ctx->stream, ctx->capturing ? cudaEventRecordExternal : 0);
     idx_ = static_cast<int>(ctx->prof.size());
     ctx->prof.push_back(ProfRec{cls, a, b, flops, bytes, m, n, k});
 }
@@ -136,7 +166,8 @@ ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes, int
 ProfScope::~ProfScope()
 {
     if (idx_ < 0) return;
-    cudaEventRecord(ctx_->prof[idx_].b, ctx_->stream);
+    cudaEventRecordWithFlags(ctx_->prof[idx_].b, ctx_->stream,
+                             ctx_->capturing ? cudaEventRecordExternal : 0);
 }
 
 static void destroy_records(std::vector<ProfRec>& v)
@@ -287,6 +318,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
     }
     cudaMemset(ctx->dev_small, 0, kSmallInts * sizeof(int));
     configure_getrf_kernels(ctx);
+    configure_tc_kernels(ctx);
     const int one = 1;  // exchange epoch starts at 1: zeroed slots never match
     cudaMemcpy(ctx->dev_small + kSmallEpoch, &one, sizeof(int), cudaMemcpyHostToDevice);
     cudaDeviceSynchronize();
@@ -303,6 +335,7 @@ hdbf_status hdbf_destroy(hdbf_handle h)
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->ws) cudaFree(h->ws);
     if (h->dev_small) cudaFree(h->dev_small);
+    if (h->mix) cudaFree(h->mix);
     delete h;
     return HDBF_STATUS_SUCCESS;
 }
@@ -492,7 +525,9 @@ const char* hdbf_profile_class_name(int cls)
     static const char* names[kNumClasses] = {"sgemm_sub_kernel", "potf2_kernel",
                                              "rlt_apply_kernel", "llu_apply_kernel",
                                              "getf2_coop_kernel", "compose_swaps_kernel",
-                                             "apply_moves", "tri_inv64_kernel", "other"};
+                                             "apply_moves", "tri_inv64_kernel",
+                                             "tc_gemm_sub_kernel", "convert16_kernels",
+                                             "ir_fp64_kernels", "other"};
     return (cls >= 0 && cls < kNumClasses) ? names[cls] : "unknown";
 }
 

@@ -1,0 +1,340 @@
+// Mixed-precision trailing update on the 5th-generation tensor cores:
+//     C (FP32, column-major, in place) -= scale * A * B^T
+// with A (M x K) and B (N x K) stored K-major in 16-bit (BF16 or FP16)
+// "shadow" copies, products accumulated in FP32 in tensor memory.
+//
+// Replaces the reference's FP16 GEMM path (launch_mixed_gemm,
+// src/gemm/mixed_gemm.cpp:8-96: rocblas_gemm_ex with FP16 inputs AND an FP16
+// C), here with an FP32 C: every trailing update is applied to the FP32
+// master matrix, only the two input operands are rounded to 16 bits.
+//
+// Kernel: one 128 x 128 output tile per CTA (4 warps).  Warp 0 / lane 0 feeds
+// a STAGES-deep shared-memory ring with TMA tile loads (128 rows x 64
+// elements of A and of B per stage, 128-byte swizzle, no multicast); warp 1 /
+// lane 0 issues tcgen05.mma (kind::f16, M=128, N=128, K=16) into a 128-column
+// TMEM accumulator and frees ring slots with tcgen05.commit; after the last
+// MMA all four warps read the accumulator back with tcgen05.ld (each warp its
+// own 32-lane TMEM sub-partition) and update C with coalesced FP32
+// read-modify-writes.  Every mbarrier wait is bounded: on expiry the kernel
+// records an error, drains what it issued, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "internal.h"
+
+namespace hdbf {
+namespace {
+
+constexpr int TM = 128;
+constexpr int TN = 128;
+constexpr int TK = 64;  // 64 x 16-bit = 128 bytes = one swizzle row
+constexpr int STAGES = 4;
+constexpr int A_BYTES = TM * TK * 2;
+constexpr int B_BYTES = TN * TK * 2;
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TMEM_COLS = 128;
+constexpr size_t kTcSmem = (size_t)STAGES * STAGE_BYTES + 1024;  // + alignment slack
+constexpr long long kWaitCycles = 4000000000LL;                   // ~2 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase; false (and *err set) on expiry.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > kWaitCycles) {
+            atomicExch(err, kErrTimeout);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), LBO unused for swizzled K-major, version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulate, A/B = BF16 (fmt 1) or
+// FP16 (fmt 0), both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t make_idesc(int fmt)
+{
+    return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((uint32_t)(TN >> 3) << 17) |
+           ((uint32_t)(TM >> 4) << 24);
+}
+
+struct TcArgs {
+    int M, N, K;
+    int a_row0, a_k0, b_row0, b_k0;
+    float* C;
+    long long ldc;
+    float scale;
+    int tiles_m;
+    int lower;
+    int fmt;
+    int* err;
+};
+
+__global__ void __launch_bounds__(128, 1)
+tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                   const TcArgs args)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[STAGES];
+    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int s_fail;
+
+    const int tm = blockIdx.x % args.tiles_m;
+    const int tn = blockIdx.x / args.tiles_m;
+    const int m0 = tm * TM, n0 = tn * TN;
+    if (args.lower && m0 + TM <= n0) return;  // tile strictly above the diagonal
+
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                               ~static_cast<uintptr_t>(1023));
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + STAGES * A_BYTES;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(&done_bar, 1);
+        s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t taddr = tmem_slot;
+    const int ktiles = (args.K + TK - 1) / TK;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int s = kt % STAGES;
+            if (kt >= STAGES && !mbar_wait(&empty_bar[s], ((kt / STAGES) - 1) & 1, args.err)) {
+                s_fail = 1;
+                break;
+            }
+            mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+            tma_load_2d(sA + s * A_BYTES, &mapA, &full_bar[s], args.a_k0 + kt * TK, args.a_row0 + m0);
+            tma_load_2d(sB + s * B_BYTES, &mapB, &full_bar[s], args.b_k0 + kt * TK, args.b_row0 + n0);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        const uint32_t idesc = make_idesc(args.fmt);
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(&full_bar[s], (kt / STAGES) & 1, args.err)) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sA + s * A_BYTES);
+            const uint32_t b0 = smem_u32(sB + s * B_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < TK / 16; ++kk) {
+                const uint64_t ad = sw128_desc(a0 + kk * 32);
+                const uint64_t bd = sw128_desc(b0 + kk * 32);
+                const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(taddr),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&empty_bar[s]))
+                : "memory");
+        }
+        // done_bar fires once every MMA issued above has completed.
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&done_bar))
+            : "memory");
+    }
+
+    __syncwarp();
+    const bool ok = mbar_wait(&done_bar, 0, args.err);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    __syncthreads();
+    if (ok && !s_fail && ktiles > 0) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t lane_base = taddr + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < TN; c0 += 32) {
+            uint32_t v[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                  "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                  "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                  "=r"(v[30]), "=r"(v[31])
+                : "r"(lane_base + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < args.M) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col < args.N && (!args.lower || row >= col)) {
+                        float* cp = args.C + (long long)col * args.ldc + row;
+                        *cp = fmaf(-args.scale, __uint_as_float(v[j]), *cp);
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr),
+                     "r"(TMEM_COLS));
+}
+
+// --------------------------------------------------------------- tensor maps
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// 2-D map over a K-major 16-bit matrix: dims (k_extent, row_extent), row
+// stride ld elements; box 64 x 128 with 128-byte swizzle; reads outside the
+// extents return zero.
+bool make_map(CUtensorMap* map, const void* base, long long ld, long long row_extent,
+              long long k_extent, int fmt)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)k_extent, (cuuint64_t)row_extent};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)TM};
+    cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapDataType dt =
+        fmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+void configure_tc_kernels(hdbf_context* ctx)
+{
+    (void)ctx;
+    cudaFuncSetAttribute(tc_gemm_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kTcSmem);
+    cudaGetLastError();
+}
+
+hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
+                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only)
+{
+    if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
+    if (!A.base || !B.base || !C) return HDBF_STATUS_INVALID_VALUE;
+    // TMA: 16-byte aligned base and row stride; the K coordinate of every
+    // tile must start on a 16-byte (8-element) boundary.
+    if ((reinterpret_cast<uintptr_t>(A.base) & 15u) || (reinterpret_cast<uintptr_t>(B.base) & 15u) ||
+        (A.ld % 8) || (B.ld % 8) || (A.k0 % 8) || (B.k0 % 8))
+        return HDBF_STATUS_INVALID_VALUE;
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, A.base, A.ld, (long long)A.row0 + M, (long long)A.k0 + K, fmt) ||
+        !make_map(&mb, B.base, B.ld, (long long)B.row0 + N, (long long)B.k0 + K, fmt))
+        return HDBF_STATUS_NOT_SUPPORTED;
+    TcArgs args;
+    args.M = M;
+    args.N = N;
+    args.K = K;
+    args.a_row0 = A.row0;
+    args.a_k0 = A.k0;
+    args.b_row0 = B.row0;
+    args.b_k0 = B.k0;
+    args.C = C;
+    args.ldc = ldc;
+    args.scale = scale;
+    args.tiles_m = (M + TM - 1) / TM;
+    args.lower = lower_only ? 1 : 0;
+    args.fmt = fmt;
+    args.err = ctx->dev_small + kSmallErr;
+    const long long grid = (long long)args.tiles_m * ((N + TN - 1) / TN);
+    if (grid > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
+    double flops = 2.0 * (double)M * N * K;
+    ProfScope prof(ctx, kClsTcGemm, flops, 2.0 * ((double)M * K + (double)N * K) + 8.0 * M * N, M,
+                   N, K);
+    tc_gemm_sub_kernel<<<(unsigned)grid, 128, kTcSmem, ctx->stream>>>(ma, mb, args);
+    ctx->launches++;
+    return last_cuda(ctx);
+}
+
+}  // namespace hdbf
