@@ -69,6 +69,7 @@ _PROTOS = {
     "recursive_syrk_parallel": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
     "batched_syrk_bottom_up": (None, [P, P, P, c_int, P, c_int, c_int, c_int, c_int]),
     "trsm_right_lower_transpose": (None, [P, c_int, c_int, P, c_int, P, c_int]),
+    "trsm_right_lower_transpose_noalloc": (c_int, [c_int, c_int, P, c_int, P, c_int, P]),
     "double_blocked_trsm": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int, c_int]),
     "recursive_trsm": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
     "recursive_trsm_tiled_update": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
