@@ -76,6 +76,17 @@ _PROTOS = {
     "iterative_trsm_right_looking": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
     "gemm_nt_update": (None, [P, c_int, c_int, c_int, P, c_int, P, c_int, P, c_int]),
     "gemm_nt_update_m_tiled": (None, [P, c_int, c_int, c_int, P, c_int, P, c_int, P, c_int, c_int]),
+    "recursive_potrf_mixed_driver": (None, [P, P, P, c_int, c_int, c_int, P]),
+    "batched_syrk_bottom_up_mixed": (None, [P, P, P, c_int, P, c_int, c_int, c_int, c_int]),
+    "recursive_trsm_mixed": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
+    "hdbf_spotrf_mixed": (c_int, [P, c_int, P, c_int, c_int, c_int, P]),
+    "hdbf_sgetrf_mixed": (c_int, [P, c_int, P, c_int, c_int, c_int, P, P]),
+    "hdbf_spotrs": (c_int, [P, P, c_int, c_int, c_int, P, c_int]),
+    "hdbf_sgetrs": (c_int, [P, P, c_int, c_int, P, c_int, P, c_int]),
+    "hdbf_dposv_mixed": (c_int, [P, c_int, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
+                                 c_double, c_int, P]),
+    "hdbf_dgesv_mixed": (c_int, [P, c_int, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
+                                 c_double, c_int, P]),
     "launch_mixed_gemm": (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_float, P, c_int, P,
                                  c_int, c_float, P, c_int]),
     # kernels
@@ -85,6 +96,16 @@ _PROTOS = {
     "launch_fp16_to_fp32": (None, [P, P, c_int, c_int, c_int, c_int, P]),
     "launch_auto_scale": (None, [P, c_int, c_int, P, ctypes.c_bool, P]),
 }
+
+
+PREC = {"fp32": 0, "bf16": 1, "fp16": 2, "bf16x3": 3, "fp16x3": 4}
+
+
+class IrInfo(ctypes.Structure):
+    """hdbf_ir_info (include/hdbf/mixed.h)."""
+    _fields_ = [("iterations", c_int), ("converged", c_int), ("final_precision", c_int),
+                ("factorizations", c_int), ("info", c_int), ("backward_error", c_double),
+                ("history", c_double * 64), ("factor_ms", c_double), ("refine_ms", c_double)]
 
 
 class HdbfError(RuntimeError):

@@ -83,6 +83,7 @@ constexpr int kSmallErr = 0;       // device error word (timeouts, invalid pivot
 constexpr int kSmallMoveCount = 12;  // move count of the last composed permutation
 constexpr int kSmallEpoch = 16;      // panel-kernel exchange epoch
 constexpr int kSmallDone = 20;       // panel-kernel finished-CTA counter
+constexpr int kSmallScratch = 24;    // host-read reduction results (absmax etc.)
 constexpr int kSmallInts = 64;
 
 // Device error codes written into dev_small[kSmallErr].
@@ -143,6 +144,10 @@ hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N,
                       const float* A, long long lda, const float* B, long long ldb,
                       float* C, long long ldc);
 
+// C(M x N) -= A^T * B with A stored K x M and B stored K x N (column-major).
+hdbf_status sgemm_sub_tn(hdbf_context* ctx, int M, int N, int K, const float* A, long long lda,
+                         const float* B, long long ldb, float* C, long long ldc);
+
 // Unblocked-in-shared-memory Cholesky of an n x n (n <= 64) diagonal block.
 hdbf_status potf2_small(hdbf_context* ctx, int n, float* A, long long lda, int* info,
                         int info_base);
@@ -157,6 +162,23 @@ hdbf_status llu_apply(hdbf_context* ctx, int rows, int cols, const float* inv, f
                       long long ldb);
 hdbf_status rlt_apply(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
                       long long ldb);
+
+// Inverse modes: 0 lower non-unit, 1 lower unit, 2 upper non-unit.
+hdbf_status tri_inv64_mode(hdbf_context* ctx, int n, const float* L, long long ldl, int mode,
+                           float* out);
+// B <- inv * B (trans=false) or inv^T * B (trans=true), rows <= 64.
+hdbf_status llu_apply_t(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
+                        long long ldb, bool trans);
+
+// Solves on FP32 factors (solves.cu).
+hdbf_status ipiv_to_perm(hdbf_context* ctx, const int* ipiv, int n, int* perm);
+hdbf_status gather_rows_perm(hdbf_context* ctx, const float* src, long long lds, float* dst,
+                             long long ldd, const int* perm, int n, int cols);
+hdbf_status potrs_f32(hdbf_context* ctx, const float* L, long long ldl, int n, int nrhs, float* B,
+                      long long ldb);
+hdbf_status getrs_f32_permuted(hdbf_context* ctx, const float* LU, long long ldlu, int n, int nrhs,
+                               float* B, long long ldb);
+void configure_solve_kernels(hdbf_context* ctx);
 
 // Cooperative partially pivoted LU of an m x w panel (w <= 32).  Pivots are
 // written 1-based as (local row + 1 + ipiv_add).

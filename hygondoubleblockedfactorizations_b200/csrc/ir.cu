@@ -1,0 +1,488 @@
+// FP64 iterative refinement around the low-precision factorizations.
+//
+// Only the refinement residual r = b - A x and the update x += d run in FP64
+// on the GPU; the correction d = A^{-1} r is solved with the FP32 factors
+// (after scaling each residual column by its infinity norm so that the FP32
+// solve never underflows).  Not part of the reference, which has no solve.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+#include "getrf/double_blocked_getrf.h"
+#include "hdbf/mixed.h"
+#include "potrf/double_blocked_potrf.h"
+
+namespace hdbf {
+
+hdbf_status potrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
+                        int* info);
+hdbf_status getrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
+                        int* ipiv, int* info);
+size_t mixed_shadow_bytes(int n, int b, bool split);
+
+namespace {
+
+constexpr int kRhsGroup = 16;
+constexpr int kSplits = 16;
+constexpr int kRowsPerCta = 256;
+constexpr int kJChunk = 32;
+
+__global__ void d2s_kernel(const double* __restrict__ A, long long lda, float* W, long long ldw,
+                           int rows, int cols)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const long long c = blockIdx.y;
+    if (r < rows && c < cols) W[c * ldw + r] = (float)A[c * lda + r];
+}
+
+// partial[s][c][r] = sum_{j in split s} A(r, j) * X(j, c) for the RHS group
+// blockIdx.z (columns 16 z .. 16 z + 15).
+__global__ void __launch_bounds__(kRowsPerCta) resid_partial_kernel(
+    const double* __restrict__ A, long long lda, const double* __restrict__ X, long long ldx, int n,
+    int nrhs, double* partial)
+{
+    __shared__ double xs[kJChunk][kRhsGroup];
+    const int r = blockIdx.x * kRowsPerCta + threadIdx.x;
+    const int s = blockIdx.y;
+    const int c0 = blockIdx.z * kRhsGroup;
+    const int nc = min(kRhsGroup, nrhs - c0);
+    const int per = (n + kSplits - 1) / kSplits;
+    const int j0 = s * per, j1 = min(n, j0 + per);
+    double acc[kRhsGroup];
+#pragma unroll
+    for (int c = 0; c < kRhsGroup; ++c) acc[c] = 0.0;
+    for (int jb = j0; jb < j1; jb += kJChunk) {
+        const int jn = min(kJChunk, j1 - jb);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < kJChunk * kRhsGroup; idx += kRowsPerCta) {
+            const int jj = idx / kRhsGroup, c = idx % kRhsGroup;
+            xs[jj][c] = (jj < jn && c < nc) ? X[(long long)(c0 + c) * ldx + jb + jj] : 0.0;
+        }
+        __syncthreads();
+        if (r < n) {
+            for (int jj = 0; jj < jn; ++jj) {
+                const double a = A[(long long)(jb + jj) * lda + r];
+#pragma unroll
+                for (int c = 0; c < kRhsGroup; ++c) acc[c] = fma(a, xs[jj][c], acc[c]);
+            }
+        }
+    }
+    if (r < n)
+        for (int c = 0; c < nc; ++c)
+            partial[((long long)s * nrhs + c0 + c) * n + r] = acc[c];
+}
+
+// R(r, c) = B(r, c) - sum_s partial[s][c][r]
+__global__ void resid_final_kernel(const double* __restrict__ partial, const double* B,
+                                   long long ldb, double* R, long long ldr, int n, int nrhs)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    double acc = 0.0;
+    for (int s = 0; s < kSplits; ++s) acc += partial[((long long)s * nrhs + c) * n + r];
+    R[(long long)c * ldr + r] = B[(long long)c * ldb + r] - acc;
+}
+
+// out[c] = max_r |V(r, c)| (non-negative doubles order like their bits)
+__global__ void colmax_kernel(const double* __restrict__ V, long long ldv, int n,
+                              unsigned long long* out)
+{
+    const int c = blockIdx.y;
+    double m = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        m = fmax(m, fabs(V[(long long)c * ldv + r]));
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + c, (unsigned long long)__double_as_longlong(m));
+}
+
+// rowsum partials for ||A||_inf: partial[s][r] = sum_{j in split s} |A(r, j)|
+__global__ void rowabs_partial_kernel(const double* __restrict__ A, long long lda, int n,
+                                      double* partial)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int s = blockIdx.y;
+    if (r >= n) return;
+    const int per = (n + kSplits - 1) / kSplits;
+    const int j0 = s * per, j1 = min(n, j0 + per);
+    double acc = 0.0;
+    for (int j = j0; j < j1; ++j) acc += fabs(A[(long long)j * lda + r]);
+    partial[(long long)s * n + r] = acc;
+}
+
+__global__ void rowabs_final_kernel(const double* __restrict__ partial, int n,
+                                    unsigned long long* out)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    double v = 0.0;
+    if (r < n)
+        for (int s = 0; s < kSplits; ++s) v += partial[(long long)s * n + r];
+    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+}
+
+// F(r, c) = (float)(V(r, c) / nrm[c])
+__global__ void scale_to_f32_kernel(const double* __restrict__ V, long long ldv,
+                                    const unsigned long long* nrm, float* F, long long ldf, int n,
+                                    int nrhs)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    const double s = __longlong_as_double((long long)nrm[c]);
+    F[(long long)c * ldf + r] = s > 0.0 ? (float)(V[(long long)c * ldv + r] / s) : 0.f;
+}
+
+// X(r, c) (+)= (double)F(r, c) * nrm[c]
+__global__ void update_x_kernel(const float* __restrict__ F, long long ldf,
+                                const unsigned long long* nrm, double* X, long long ldx, int n,
+                                int nrhs, int accumulate)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    const double s = __longlong_as_double((long long)nrm[c]);
+    const double d = (double)F[(long long)c * ldf + r] * s;
+    double* x = X + (long long)c * ldx + r;
+    *x = accumulate ? *x + d : d;
+}
+
+struct IrBuffers {
+    float* W = nullptr;      // FP32 working copy / factors (n x n, ld n)
+    int* ipiv = nullptr;
+    int* perm = nullptr;
+    int* info = nullptr;
+    double* R = nullptr;     // n x nrhs residual
+    float* F = nullptr;      // n x nrhs scaled FP32 right-hand side / correction
+    float* F2 = nullptr;     // permuted copy for GETRS
+    double* part = nullptr;  // kSplits x nrhs x n partial sums
+    unsigned long long* nrm = nullptr;  // [0, nrhs): column norms; [nrhs]: ||A||_inf
+};
+
+inline size_t al(size_t x) { return (x + 255) / 256 * 256; }
+
+size_t ir_bytes(int n, int nrhs)
+{
+    return al((size_t)n * n * 4) + 3 * al((size_t)n * 4) + al(64) + al((size_t)n * nrhs * 8) +
+           2 * al((size_t)n * nrhs * 4) + al((size_t)kSplits * nrhs * n * 8) +
+           al((size_t)(nrhs + 1) * 8) + 4096;
+}
+
+IrBuffers carve(char* base, int n, int nrhs)
+{
+    IrBuffers b;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* p = base + off;
+        off += al(bytes);
+        return p;
+    };
+    b.W = reinterpret_cast<float*>(take((size_t)n * n * 4));
+    b.ipiv = reinterpret_cast<int*>(take((size_t)n * 4));
+    b.perm = reinterpret_cast<int*>(take((size_t)n * 4));
+    take((size_t)n * 4);
+    b.info = reinterpret_cast<int*>(take(64));
+    b.R = reinterpret_cast<double*>(take((size_t)n * nrhs * 8));
+    b.F = reinterpret_cast<float*>(take((size_t)n * nrhs * 4));
+    b.F2 = reinterpret_cast<float*>(take((size_t)n * nrhs * 4));
+    b.part = reinterpret_cast<double*>(take((size_t)kSplits * nrhs * n * 8));
+    b.nrm = reinterpret_cast<unsigned long long*>(take((size_t)(nrhs + 1) * 8));
+    return b;
+}
+
+int next_precision(int prec)
+{
+    switch (prec) {
+    case HDBF_PREC_BF16: return HDBF_PREC_BF16X3;
+    case HDBF_PREC_FP16: return HDBF_PREC_FP16X3;
+    case HDBF_PREC_BF16X3:
+    case HDBF_PREC_FP16X3: return HDBF_PREC_FP32;
+    default: return -1;
+    }
+}
+
+class IrSolver {
+public:
+    IrSolver(hdbf_context* ctx, bool spd, const double* A, long long lda, int n, int nrhs,
+             const double* B, long long ldb, double* X, long long ldx, const IrBuffers& buf)
+        : ctx_(ctx), spd_(spd), A_(A), lda_(lda), n_(n), nrhs_(nrhs), B_(B), ldb_(ldb), X_(X),
+          ldx_(ldx), b_(buf) {}
+
+    hdbf_status factor(int prec, int* host_info)
+    {
+        cudaStream_t s = ctx_->stream;
+        dim3 g((n_ + 255) / 256, n_);
+        d2s_kernel<<<g, 256, 0, s>>>(A_, lda_, b_.W, n_, n_, n_);
+        ctx_->launches++;
+        HDBF_TRY(last_cuda(ctx_));
+        const int nb = 512;
+        if (prec == HDBF_PREC_FP32) {
+            if (spd_) double_blocked_potrf_kblocked_syrk(ctx_, b_.W, n_, n_, 4096, nb, 0, b_.info);
+            else double_blocked_getrf(ctx_, b_.W, n_, n_, 8192, nb, getrf_outer_trsm_direct, 0,
+                                      b_.ipiv, b_.info);
+            HDBF_TRY(ctx_->last_status);
+        } else if (spd_) {
+            HDBF_TRY(potrf_mixed(ctx_, prec, b_.W, n_, n_, nb, b_.info));
+        } else {
+            HDBF_TRY(getrf_mixed(ctx_, prec, b_.W, n_, n_, nb, b_.ipiv, b_.info));
+        }
+        if (!spd_) HDBF_TRY(ipiv_to_perm(ctx_, b_.ipiv, n_, b_.perm));
+        if (cudaMemcpyAsync(host_info, b_.info, sizeof(int), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            cudaGetLastError();
+            return HDBF_STATUS_CUDA_ERROR;
+        }
+        return HDBF_STATUS_SUCCESS;
+    }
+
+    // d = A^{-1} v with the FP32 factors; v scaled column-wise by nrm.
+    hdbf_status correction(const double* V, long long ldv, bool accumulate)
+    {
+        cudaStream_t s = ctx_->stream;
+        HDBF_TRY(colmax(V, ldv, b_.nrm));
+        dim3 g((n_ + 255) / 256, nrhs_);
+        scale_to_f32_kernel<<<g, 256, 0, s>>>(V, ldv, b_.nrm, b_.F, n_, n_, nrhs_);
+        ctx_->launches++;
+        float* sol = b_.F;
+        if (spd_) {
+            HDBF_TRY(potrs_f32(ctx_, b_.W, n_, n_, nrhs_, b_.F, n_));
+        } else {
+            HDBF_TRY(gather_rows_perm(ctx_, b_.F, n_, b_.F2, n_, b_.perm, n_, nrhs_));
+            HDBF_TRY(getrs_f32_permuted(ctx_, b_.W, n_, n_, nrhs_, b_.F2, n_));
+            sol = b_.F2;
+        }
+        update_x_kernel<<<g, 256, 0, s>>>(sol, n_, b_.nrm, X_, ldx_, n_, nrhs_, accumulate ? 1 : 0);
+        ctx_->launches++;
+        return last_cuda(ctx_);
+    }
+
+    hdbf_status residual()
+    {
+        cudaStream_t s = ctx_->stream;
+        dim3 g1((n_ + kRowsPerCta - 1) / kRowsPerCta, kSplits, (nrhs_ + kRhsGroup - 1) / kRhsGroup);
+        ProfScope prof(ctx_, kClsIr, 2.0 * (double)n_ * n_ * nrhs_, 8.0 * (double)n_ * n_);
+        resid_partial_kernel<<<g1, kRowsPerCta, 0, s>>>(A_, lda_, X_, ldx_, n_, nrhs_, b_.part);
+        dim3 g2((n_ + 255) / 256, nrhs_);
+        resid_final_kernel<<<g2, 256, 0, s>>>(b_.part, B_, ldb_, b_.R, n_, n_, nrhs_);
+        ctx_->launches += 2;
+        return last_cuda(ctx_);
+    }
+
+    hdbf_status colmax(const double* V, long long ldv, unsigned long long* out)
+    {
+        cudaMemsetAsync(out, 0, (size_t)nrhs_ * 8, ctx_->stream);
+        dim3 g(64, nrhs_);
+        colmax_kernel<<<g, 256, 0, ctx_->stream>>>(V, ldv, n_, out);
+        ctx_->launches++;
+        return last_cuda(ctx_);
+    }
+
+    hdbf_status host_colmax(const double* V, long long ldv, double* out)
+    {
+        HDBF_TRY(colmax(V, ldv, b_.nrm));
+        if (cudaMemcpyAsync(out, b_.nrm, (size_t)nrhs_ * 8, cudaMemcpyDeviceToHost,
+                            ctx_->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx_->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return HDBF_STATUS_CUDA_ERROR;
+        }
+        return HDBF_STATUS_SUCCESS;
+    }
+
+    hdbf_status anorm(double* out)
+    {
+        dim3 g((n_ + 255) / 256, kSplits);
+        rowabs_partial_kernel<<<g, 256, 0, ctx_->stream>>>(A_, lda_, n_, b_.part);
+        cudaMemsetAsync(b_.nrm + nrhs_, 0, 8, ctx_->stream);
+        rowabs_final_kernel<<<(n_ + 255) / 256, 256, 0, ctx_->stream>>>(b_.part, n_,
+                                                                          b_.nrm + nrhs_);
+        ctx_->launches += 2;
+        unsigned long long bits = 0;
+        if (cudaMemcpyAsync(&bits, b_.nrm + nrhs_, 8, cudaMemcpyDeviceToHost, ctx_->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(ctx_->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return HDBF_STATUS_CUDA_ERROR;
+        }
+        memcpy(out, &bits, 8);
+        return HDBF_STATUS_SUCCESS;
+    }
+
+    const IrBuffers& buffers() const { return b_; }
+
+private:
+    hdbf_context* ctx_;
+    bool spd_;
+    const double* A_;
+    long long lda_;
+    int n_, nrhs_;
+    const double* B_;
+    long long ldb_;
+    double* X_;
+    long long ldx_;
+    IrBuffers b_;
+};
+
+hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const double* A,
+                      int lda, int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                      double tol, int max_iter, hdbf_ir_info* out)
+{
+    hdbf_ir_info info;
+    memset(&info, 0, sizeof(info));
+    if (n < 0 || nrhs < 0 || nrhs > 64) return HDBF_STATUS_INVALID_VALUE;
+    if (n == 0 || nrhs == 0) {
+        info.converged = 1;
+        if (out) *out = info;
+        return HDBF_STATUS_SUCCESS;
+    }
+    if (!A || !B || !X || lda < n || ldb < n || ldx < n) return HDBF_STATUS_INVALID_VALUE;
+    if (prec < HDBF_PREC_FP32 || prec > HDBF_PREC_FP16X3) return HDBF_STATUS_INVALID_VALUE;
+    if (max_iter < 0) max_iter = 0;
+    HDBF_TRY(ensure_ws(ctx, n));
+    // One arena for the shadows (offset 0) and the refinement buffers.
+    const size_t shadow = mixed_shadow_bytes(n, 512, true);
+    hdbf_status st;
+    char* arena = static_cast<char*>(mixed_arena(ctx, shadow + ir_bytes(n, nrhs), &st));
+    if (!arena) return st;
+    IrSolver solver(ctx, spd, A, lda, n, nrhs, B, ldb, X, ldx,
+                    carve(arena + al(shadow), n, nrhs));
+
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto timed = [&](double* acc, auto&& fn) -> hdbf_status {
+        cudaEventRecord(e0, ctx->stream);
+        const hdbf_status s2 = fn();
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        *acc += ms;
+        return s2;
+    };
+
+    double anorm = 0.0;
+    std::vector<double> bnorm(nrhs), rnorm(nrhs), xnorm(nrhs);
+    st = solver.anorm(&anorm);
+    if (st == HDBF_STATUS_SUCCESS) st = solver.host_colmax(B, ldb, bnorm.data());
+    int cur = prec;
+    if (st == HDBF_STATUS_SUCCESS) {
+        int hinfo = 0;
+        st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
+        info.factorizations = 1;
+        while (st == HDBF_STATUS_SUCCESS && hinfo != 0 && escalate && next_precision(cur) >= 0) {
+            cur = next_precision(cur);  // FP32-panel fallback on a failed factorization
+            st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
+            info.factorizations++;
+        }
+        info.info = hinfo;
+        if (st == HDBF_STATUS_SUCCESS && hinfo == 0)
+            st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });
+        double prev = INFINITY;
+        int stalls = 0;
+        for (int it = 0; st == HDBF_STATUS_SUCCESS && hinfo == 0; ++it) {
+            st = timed(&info.refine_ms, [&] { return solver.residual(); });
+            if (st != HDBF_STATUS_SUCCESS) break;
+            st = solver.host_colmax(solver.buffers().R, n, rnorm.data());
+            if (st == HDBF_STATUS_SUCCESS) st = solver.host_colmax(X, ldx, xnorm.data());
+            if (st != HDBF_STATUS_SUCCESS) break;
+            double berr = 0.0;
+            for (int c = 0; c < nrhs; ++c) {
+                const double den = anorm * xnorm[c] + bnorm[c];
+                const double e = den > 0.0 ? rnorm[c] / den : (rnorm[c] > 0.0 ? INFINITY : 0.0);
+                berr = std::max(berr, std::isfinite(e) ? e : INFINITY);
+            }
+            if (it < HDBF_IR_HISTORY) info.history[it] = berr;
+            info.backward_error = berr;
+            info.iterations = it;
+            if (berr <= tol) {
+                info.converged = 1;
+                break;
+            }
+            if (it >= max_iter) break;
+            if (!(berr < 0.5 * prev)) {
+                if (escalate && next_precision(cur) >= 0) {
+                    cur = next_precision(cur);
+                    int hinfo2 = 0;
+                    st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo2); });
+                    info.factorizations++;
+                    info.info = hinfo2;
+                    if (hinfo2 != 0) break;
+                    stalls = 0;
+                } else if (++stalls >= 2) {
+                    break;
+                }
+            }
+            prev = std::min(prev, berr);
+            st = timed(&info.refine_ms, [&] { return solver.correction(solver.buffers().R, n, true); });
+        }
+    }
+    info.final_precision = cur;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (out) *out = info;
+    return st;
+}
+
+}  // namespace
+}  // namespace hdbf
+
+using namespace hdbf;
+
+extern "C" {
+
+hdbf_status hdbf_spotrs(hdbf_handle h, const float* L, int lda, int n, int nrhs, float* B, int ldb)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    if (n < 0 || nrhs < 0 || (n > 0 && (!L || !B || lda < n || ldb < n)))
+        return h->last_status = HDBF_STATUS_INVALID_VALUE;
+    return h->last_status = potrs_f32(h, L, lda, n, nrhs, B, ldb);
+}
+
+hdbf_status hdbf_sgetrs(hdbf_handle h, const float* LU, int lda, int n, const int* ipiv, int nrhs,
+                        float* B, int ldb)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    if (n < 0 || nrhs < 0 || (n > 0 && (!LU || !B || !ipiv || lda < n || ldb < n)))
+        return h->last_status = HDBF_STATUS_INVALID_VALUE;
+    if (n == 0 || nrhs == 0) return h->last_status = HDBF_STATUS_SUCCESS;
+    hdbf_status st = ensure_ws(h, n);
+    if (st != HDBF_STATUS_SUCCESS) return h->last_status = st;
+    const size_t need = al((size_t)n * 4) + al((size_t)n * nrhs * 4);
+    char* arena = static_cast<char*>(mixed_arena(h, need, &st));
+    if (!arena) return h->last_status = st;
+    int* perm = reinterpret_cast<int*>(arena);
+    float* tmp = reinterpret_cast<float*>(arena + al((size_t)n * 4));
+    st = ipiv_to_perm(h, ipiv, n, perm);
+    if (st == HDBF_STATUS_SUCCESS) st = gather_rows_perm(h, B, ldb, tmp, n, perm, n, nrhs);
+    if (st == HDBF_STATUS_SUCCESS) st = getrs_f32_permuted(h, LU, lda, n, nrhs, tmp, n);
+    if (st == HDBF_STATUS_SUCCESS)
+        st = cudaMemcpy2DAsync(B, (size_t)ldb * 4, tmp, (size_t)n * 4, (size_t)n * 4, nrhs,
+                               cudaMemcpyDeviceToDevice, h->stream) == cudaSuccess
+                 ? HDBF_STATUS_SUCCESS
+                 : HDBF_STATUS_CUDA_ERROR;
+    return h->last_status = st;
+}
+
+hdbf_status hdbf_dposv_mixed(hdbf_handle h, hdbf_precision prec, int escalate, const double* A,
+                             int lda, int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                             double tol, int max_iter, hdbf_ir_info* out)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = xsv_mixed(h, true, (int)prec, escalate, A, lda, n, nrhs, B, ldb, X,
+                                      ldx, tol, max_iter, out);
+}
+
+hdbf_status hdbf_dgesv_mixed(hdbf_handle h, hdbf_precision prec, int escalate, const double* A,
+                             int lda, int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                             double tol, int max_iter, hdbf_ir_info* out)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = xsv_mixed(h, false, (int)prec, escalate, A, lda, n, nrhs, B, ldb, X,
+                                      ldx, tol, max_iter, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,365 @@
+// Mixed-precision factorizations: FP32 panels, tensor-core trailing updates.
+//
+// Cholesky and LU run right-looking with block b: the diagonal block / tall
+// panel is factored in FP32 by the same kernels as the FP32 path (potf2 +
+// inverted-block TRSM; cooperative pivoted panel + device-composed row swaps),
+// the off-diagonal panel(s) are rounded once into K-major 16-bit shadows, and
+// the O(n^3) trailing update A22 -= L21 L21^T (SYRK, lower) or A22 -= L21 U12
+// runs on tcgen05 with FP32 accumulation straight into the FP32 matrix.  In
+// the split modes each operand is carried as hi + lo (lo = round(x - hi)) and
+// the update uses hi*hi + hi*lo + lo*hi.
+//
+// Reference: the mixed recursive Cholesky (src/potrf/recursive_potrf.cpp:
+// 241-388) rounds C to FP16 in every GEMM (src/gemm/mixed_gemm.cpp:53-89);
+// here C never leaves FP32.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+#include "hdbf/mixed.h"
+#include "kernels/add_damping.h"
+#include "potrf/recursive_potrf.h"
+#include "syrk/batched_syrk.h"
+#include "trsm/recursive_trsm.h"
+
+namespace hdbf {
+
+namespace {
+
+inline long long pad8(long long x) { return (x + 7) / 8 * 8; }
+inline long long fbits(float f)
+{
+    unsigned int u;
+    memcpy(&u, &f, sizeof(u));
+    return (long long)u;
+}
+inline float* at(float* A, long long lda, int r, int c) { return A + (long long)c * lda + r; }
+
+struct PrecInfo {
+    int fmt;
+    bool split;
+};
+
+PrecInfo prec_info(int prec)
+{
+    switch (prec) {
+    case HDBF_PREC_BF16: return {kFmtBF16, false};
+    case HDBF_PREC_FP16: return {kFmtF16, false};
+    case HDBF_PREC_BF16X3: return {kFmtBF16, true};
+    case HDBF_PREC_FP16X3: return {kFmtF16, true};
+    default: return {-1, false};
+    }
+}
+
+// C -= scale * (A B^T) with optional hi/lo split operands.
+hdbf_status tc_update(hdbf_context* ctx, const PrecInfo& pi, int M, int N, int K, const void* ah,
+                      const void* al, long long lda, const void* bh, const void* bl, long long ldb,
+                      float* C, long long ldc, float scale, bool lower)
+{
+    TcOperand a, b;
+    a.base = ah;
+    a.ld = lda;
+    b.base = bh;
+    b.ld = ldb;
+    HDBF_TRY(tc_gemm_sub(ctx, pi.fmt, M, N, K, a, b, C, ldc, scale, lower));
+    if (!pi.split) return HDBF_STATUS_SUCCESS;
+    TcOperand alo = a, blo = b;
+    alo.base = al;
+    blo.base = bl;
+    HDBF_TRY(tc_gemm_sub(ctx, pi.fmt, M, N, K, a, blo, C, ldc, scale, lower));
+    return tc_gemm_sub(ctx, pi.fmt, M, N, K, alo, b, C, ldc, scale, lower);
+}
+
+__global__ void absmax_kernel(const float* A, long long lda, int rows, int cols, int diag_only,
+                              unsigned int* out)
+{
+    float v = 0.f;
+    if (diag_only) {
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < rows;
+             i += (long long)gridDim.x * blockDim.x)
+            v = fmaxf(v, fabsf(A[i * lda + i]));
+    } else {
+        const long long total = (long long)rows * cols;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+             i += (long long)gridDim.x * blockDim.x)
+            v = fmaxf(v, fabsf(A[(i / rows) * lda + i % rows]));
+    }
+    for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(v));
+}
+
+}  // namespace
+
+// max |A| (diag_only: max |A(i,i)|); synchronises the stream.
+hdbf_status absmax_host(hdbf_context* ctx, const float* A, long long lda, int rows, int cols,
+                        bool diag_only, float* out)
+{
+    unsigned int* d = reinterpret_cast<unsigned int*>(ctx->dev_small + kSmallScratch);
+    cudaMemsetAsync(d, 0, sizeof(unsigned int), ctx->stream);
+    absmax_kernel<<<1184, 256, 0, ctx->stream>>>(A, lda, rows, cols, diag_only ? 1 : 0, d);
+    ctx->launches++;
+    unsigned int bits = 0;
+    if (cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    float f;
+    memcpy(&f, &bits, sizeof(f));
+    *out = f;
+    return HDBF_STATUS_SUCCESS;
+}
+
+// Power-of-two scale putting max|x| * s near 2^8 (FP16 range); 1 for BF16.
+float shadow_scale(int fmt, float maxabs)
+{
+    if (fmt != kFmtF16 || !(maxabs > 0.f) || !std::isfinite(maxabs)) return 1.f;
+    const int e = (int)std::lround(std::log2(256.0 / (double)maxabs));
+    return std::ldexp(1.f, std::max(-60, std::min(60, e)));
+}
+
+size_t mixed_shadow_bytes(int n, int b, bool split)
+{
+    return (size_t)(split ? 4 : 2) * (size_t)n * pad8(b) * 2 + 1024;
+}
+
+// Right-looking mixed Cholesky (lower) with block b; shadows in `arena`.
+hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
+                             int* info, float s, char* arena)
+{
+    const PrecInfo pi = prec_info(prec);
+    if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
+    const long long lds = pad8(b);
+    const size_t one = (size_t)n * lds * 2;
+    void* hi = arena;
+    void* lo = pi.split ? arena + one : nullptr;
+    const float inv_s2 = 1.f / (s * s);
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+    for (int k = 0; k < n; k += b) {
+        const int psz = std::min(b, n - k);
+        const int tr = n - k - psz;
+        float* Akk = at(A, lda, k, k);
+        HDBF_TRY(potrf_diag(ctx, psz, Akk, lda, info, k));
+        if (tr <= 0) continue;
+        float* A21 = at(A, lda, k + psz, k);
+        HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
+        HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, s));
+        HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
+                           at(A, lda, k + psz, k + psz), lda, inv_s2, true));
+    }
+    return last_cuda(ctx);
+}
+
+// Right-looking mixed LU with partial pivoting and block b.
+hdbf_status getrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
+                             int* ipiv, int* info, float sL, float sU, char* arena)
+{
+    const PrecInfo pi = prec_info(prec);
+    if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
+    GetrfWs ws;
+    HDBF_TRY(getrf_workspace(ctx, n, &ws));
+    const long long lds = pad8(b);
+    const size_t one = (size_t)n * lds * 2;
+    void* hL = arena;
+    void* hU = arena + one;
+    void* lL = pi.split ? arena + 2 * one : nullptr;
+    void* lU = pi.split ? arena + 3 * one : nullptr;
+    const float inv_s = 1.f / (sL * sU);
+    if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+    for (int p = 0; p < n; p += b) {
+        const int psz = std::min(b, n - p);
+        const int next = p + psz;
+        const int tr = n - next;
+        HDBF_TRY(getrf_panel(ctx, n - p, psz, at(A, lda, p, p), lda, ipiv + p, p, info, p, true,
+                             ws));
+        // this panel's row interchanges on every other column
+        HDBF_TRY(compose_swaps(ctx, ipiv + p, psz, p, n - p, ws.src, ws.tgt, ws.count, ws.gperm,
+                               info));
+        const int max_moves = std::min(n - p, 2 * psz);
+        if (p > 0)
+            HDBF_TRY(apply_moves(ctx, at(A, lda, p, 0), lda, p, ws.src, ws.tgt, ws.count,
+                                 max_moves, ws.temp, ws.temp_cols));
+        if (tr <= 0) continue;
+        HDBF_TRY(apply_moves(ctx, at(A, lda, p, next), lda, tr, ws.src, ws.tgt, ws.count,
+                             max_moves, ws.temp, ws.temp_cols));
+        HDBF_TRY(trsm_llu(ctx, psz, tr, at(A, lda, p, p), lda, at(A, lda, p, next), lda));
+        HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, at(A, lda, next, p), lda, hL, lL, lds,
+                                     sL));
+        HDBF_TRY(convert_direct16(ctx, pi.fmt, psz, tr, at(A, lda, p, next), lda, hU, lU, lds, sU));
+        HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hL, lL, lds, hU, lU, lds, at(A, lda, next, next),
+                           lda, inv_s, false));
+    }
+    return last_cuda(ctx);
+}
+
+hdbf_status potrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
+                        int* info)
+{
+    if (n < 0 || (n > 0 && (!A || lda < n))) return HDBF_STATUS_INVALID_VALUE;
+    if (n == 0) return HDBF_STATUS_SUCCESS;
+    const PrecInfo pi = prec_info(prec);
+    if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
+    if (b <= 0) b = 512;
+    b = std::min(b, n);
+    HDBF_TRY(ensure_ws(ctx, n));
+    float maxdiag = 1.f;
+    if (pi.fmt == kFmtF16) HDBF_TRY(absmax_host(ctx, A, lda, n, n, true, &maxdiag));
+    const float s = shadow_scale(pi.fmt, std::sqrt(maxdiag));  // |L| <= sqrt(max a_ii)
+    hdbf_status st;
+    char* arena = static_cast<char*>(mixed_arena(ctx, mixed_shadow_bytes(n, b, pi.split), &st));
+    if (!arena) return st;
+    const std::vector<long long> key = {30, prec, (long long)A, lda, n, b, (long long)info,
+                                        fbits(s), (long long)arena};
+    return run_graph(ctx, key, [&] { return potrf_mixed_body(ctx, prec, A, lda, n, b, info, s, arena); });
+}
+
+hdbf_status getrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
+                        int* ipiv, int* info)
+{
+    if (n < 0 || (n > 0 && (!A || lda < n || !ipiv))) return HDBF_STATUS_INVALID_VALUE;
+    if (n == 0) return HDBF_STATUS_SUCCESS;
+    const PrecInfo pi = prec_info(prec);
+    if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
+    if (b <= 0) b = 512;
+    b = std::min(b, n);
+    HDBF_TRY(ensure_ws(ctx, n));
+    float maxa = 1.f;
+    if (pi.fmt == kFmtF16) HDBF_TRY(absmax_host(ctx, A, lda, n, n, false, &maxa));
+    const float sL = 1.f;  // |L| <= 1 under partial pivoting
+    const float sU = shadow_scale(pi.fmt, 8.f * maxa);  // headroom for element growth
+    hdbf_status st;
+    char* arena = static_cast<char*>(mixed_arena(ctx, mixed_shadow_bytes(n, b, pi.split), &st));
+    if (!arena) return st;
+    const std::vector<long long> key = {31, prec, (long long)A, lda, n, b, (long long)ipiv,
+                                        (long long)info, fbits(sU),
+                                        (long long)arena};
+    return run_graph(ctx, key, [&] {
+        return getrf_mixed_body(ctx, prec, A, lda, n, b, ipiv, info, sL, sU, arena);
+    });
+}
+
+}  // namespace hdbf
+
+using namespace hdbf;
+
+extern "C" {
+
+hdbf_status hdbf_spotrf_mixed(hdbf_handle h, hdbf_precision prec, float* A, int lda, int n, int nb,
+                              int* info)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = potrf_mixed(h, (int)prec, A, lda, n, nb, info);
+}
+
+hdbf_status hdbf_sgetrf_mixed(hdbf_handle h, hdbf_precision prec, float* A, int lda, int n, int nb,
+                              int* ipiv, int* info)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = getrf_mixed(h, (int)prec, A, lda, n, nb, ipiv, info);
+}
+
+// Reference recursive_potrf_mixed_driver (src/potrf/recursive_potrf.cpp:
+// 350-388): FP16 products with the reference's damping retry at failure
+// (lambda0 = 1e-4 * max|a_ii| -- 6.55 on the reference's 65504-scaled
+// matrix --, doubled, at most 5 attempts).  The FP16 range is handled by the
+// shadow scale, so the matrix itself is not rescaled.
+void recursive_potrf_mixed_driver(hdbf_handle h, StreamPool* pool, float* A, int lda, int n,
+                                  int nb, int* info)
+{
+    (void)pool;
+    if (!h) return;
+    if (n < 0 || (n > 0 && (!A || lda < n))) { h->last_status = HDBF_STATUS_INVALID_VALUE; return; }
+    if (n == 0) { h->last_status = HDBF_STATUS_SUCCESS; return; }
+    const size_t bytes = (size_t)n * n * sizeof(float);
+    hdbf_status st = ensure_ws(h, n);
+    if (st != HDBF_STATUS_SUCCESS) { h->last_status = st; return; }
+    float maxdiag = 0.f;
+    st = absmax_host(h, A, lda, n, n, true, &maxdiag);
+    if (st != HDBF_STATUS_SUCCESS) { h->last_status = st; return; }
+    // Backup of A for the damping retries (kept out of the mixed arena,
+    // which the factorization uses for its shadows).
+    float* backup = nullptr;
+    if (cudaMalloc(&backup, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        h->last_status = HDBF_STATUS_ALLOC_FAILED;
+        return;
+    }
+    cudaMemcpy2DAsync(backup, (size_t)n * 4, A, (size_t)lda * 4, (size_t)n * 4, n,
+                      cudaMemcpyDeviceToDevice, h->stream);
+    float lambda = 1e-4f * maxdiag;
+    for (int attempt = 0; attempt <= 5; ++attempt) {
+        if (attempt > 0) {
+            cudaMemcpy2DAsync(A, (size_t)lda * 4, backup, (size_t)n * 4, (size_t)n * 4, n,
+                              cudaMemcpyDeviceToDevice, h->stream);
+            launch_add_damping(A, n, lda, lambda, h->stream);
+            lambda *= 2.f;
+        }
+        st = potrf_mixed(h, HDBF_PREC_FP16, A, lda, n, nb > 0 ? nb : 512, info);
+        if (st != HDBF_STATUS_SUCCESS) break;
+        int hinfo = 0;
+        cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        cudaStreamSynchronize(h->stream);
+        if (hinfo <= 0) break;
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaFree(backup);
+    h->last_status = st;
+}
+
+void batched_syrk_bottom_up_mixed(hdbf_handle h, StreamPool* pool, float* A, int lda, float* C,
+                                  int ldc, int n, int k, int nb)
+{
+    (void)pool;
+    (void)nb;
+    if (!h) return;
+    if (n <= 0 || k <= 0) { h->last_status = HDBF_STATUS_SUCCESS; return; }
+    if (!A || !C || lda < n || ldc < n) { h->last_status = HDBF_STATUS_INVALID_VALUE; return; }
+    const long long kp = pad8(k);
+    hdbf_status st;
+    char* arena = static_cast<char*>(mixed_arena(h, (size_t)n * kp * 2 + 256, &st));
+    if (!arena) { h->last_status = st; return; }
+    const PrecInfo pi = {kFmtF16, false};
+    st = convert_transpose16(h, kFmtF16, n, k, A, lda, arena, nullptr, kp, 1.f);
+    if (st == HDBF_STATUS_SUCCESS)
+        st = tc_update(h, pi, n, n, k, arena, nullptr, kp, arena, nullptr, kp, C, ldc, 1.f, true);
+    h->last_status = st;
+}
+
+// B (n x m) <- B * A^{-T}: recursion on column halves down to nb (FP32
+// leaves), the update B2 -= X1 L21^T on FP16 tensor cores.
+static hdbf_status rec_trsm_mixed(hdbf_context* ctx, const float* L, long long ldl, float* B,
+                                  long long ldb, int n, int m, int nb, char* arena)
+{
+    if (n <= 0 || m <= 0) return HDBF_STATUS_SUCCESS;
+    if (m <= nb || nb <= 0) return trsm_rlt(ctx, n, m, L, ldl, B, ldb);
+    const int m1 = m / 2, m2 = m - m1;
+    HDBF_TRY(rec_trsm_mixed(ctx, L, ldl, B, ldb, n, m1, nb, arena));
+    const long long kp = pad8(m1);
+    void* xs = arena;
+    void* ls = arena + (size_t)n * kp * 2;
+    HDBF_TRY(convert_transpose16(ctx, kFmtF16, n, m1, B, ldb, xs, nullptr, kp, 1.f));
+    HDBF_TRY(convert_transpose16(ctx, kFmtF16, m2, m1, L + m1, ldl, ls, nullptr, kp, 1.f));
+    const PrecInfo pi = {kFmtF16, false};
+    HDBF_TRY(tc_update(ctx, pi, n, m2, m1, xs, nullptr, kp, ls, nullptr, kp, B + (long long)m1 * ldb,
+                       ldb, 1.f, false));
+    return rec_trsm_mixed(ctx, L + (long long)m1 * ldl + m1, ldl, B + (long long)m1 * ldb, ldb, n,
+                          m2, nb, arena);
+}
+
+void recursive_trsm_mixed(hdbf_handle h, float* A, int lda, float* B, int ldb, int n, int m, int nb)
+{
+    if (!h) return;
+    if (n <= 0 || m <= 0) { h->last_status = HDBF_STATUS_SUCCESS; return; }
+    if (!A || !B || lda < m || ldb < n) { h->last_status = HDBF_STATUS_INVALID_VALUE; return; }
+    hdbf_status st = ensure_ws(h, std::max(n, m));
+    if (st != HDBF_STATUS_SUCCESS) { h->last_status = st; return; }
+    const size_t need = (size_t)(n + m) * pad8(m) * 2 + 1024;
+    char* arena = static_cast<char*>(mixed_arena(h, need, &st));
+    if (!arena) { h->last_status = st; return; }
+    h->last_status = rec_trsm_mixed(h, A, lda, B, ldb, n, m, nb, arena);
+}
+
+}  // extern "C"

@@ -88,16 +88,23 @@ __global__ void __launch_bounds__(256) potf2_kernel(int n, float* A, long long l
 // L_bb x = e_t by forward substitution (right-looking, so every L read is a
 // shared-memory broadcast).  out[b*4096 + c*64 + r] = inv(L_bb)(r, c); a
 // partial last block is padded with the identity.
+// mode 0: lower non-unit, 1: lower unit, 2: upper non-unit (the upper block
+// U is inverted as (U^T)^{-1} and stored transposed).
 __global__ void __launch_bounds__(kLeaf) tri_inv64_kernel(int n, const float* __restrict__ L,
-                                                          long long ldl, int unit, float* out)
+                                                          long long ldl, int mode, float* out)
 {
-    __shared__ float Ls[kLeaf][kLeaf + 1];  // Ls[r][c] = L(base + r, base + c)
+    __shared__ float Ls[kLeaf][kLeaf + 1];  // Ls[r][c] = T(base + r, base + c), T lower
     const int base = blockIdx.x * kLeaf;
     const int nb = min(kLeaf, n - base);
     const int t = threadIdx.x;
+    const int unit = mode == 1;
     for (int idx = t; idx < kLeaf * kLeaf; idx += kLeaf) {
         const int c = idx / kLeaf, r = idx - c * kLeaf;
-        Ls[r][c] = (r < nb && c < nb && r >= c) ? L[(long long)(base + c) * ldl + base + r] : 0.f;
+        float v = 0.f;
+        if (r < nb && c < nb && r >= c)
+            v = mode == 2 ? L[(long long)(base + r) * ldl + base + c]
+                          : L[(long long)(base + c) * ldl + base + r];
+        Ls[r][c] = v;
     }
     __syncthreads();
     float x[kLeaf];
@@ -111,16 +118,21 @@ __global__ void __launch_bounds__(kLeaf) tri_inv64_kernel(int n, const float* __
             for (int i = k + 1; i < kLeaf; ++i) x[i] = fmaf(-Ls[i][k], x[k], x[i]);
         }
     }
-    float* o = out + (long long)blockIdx.x * kLeaf * kLeaf + (long long)t * kLeaf;
+    float* ob = out + (long long)blockIdx.x * kLeaf * kLeaf;
+    if (mode == 2) {
 #pragma unroll
-    for (int i = 0; i < kLeaf; ++i) o[i] = x[i];
+        for (int i = 0; i < kLeaf; ++i) ob[(long long)i * kLeaf + t] = x[i];  // row t of U^{-1}
+    } else {
+#pragma unroll
+        for (int i = 0; i < kLeaf; ++i) ob[(long long)t * kLeaf + i] = x[i];  // column t
+    }
 }
 
 // B(rows x cols) <- inv * B for rows <= 64 (inv = L^{-1} of the leaf block):
 // CTA = 64 x 64 tile of B, thread = 4 x 4 outputs, in place.
 __global__ void __launch_bounds__(256) llu_apply_kernel(int rows, int cols,
                                                         const float* __restrict__ inv, float* B,
-                                                        long long ldb)
+                                                        long long ldb, int trans)
 {
     __shared__ __align__(16) float Is[kLeaf][kLeaf];  // Is[k][r] = inv(r, k)
     __shared__ __align__(16) float Bs[kLeaf][kLeaf];  // Bs[k][c] = B(k, c0 + c)
@@ -128,7 +140,7 @@ __global__ void __launch_bounds__(256) llu_apply_kernel(int rows, int cols,
     const long long c0 = (long long)blockIdx.x * kLeaf;
     for (int idx = tid; idx < kLeaf * kLeaf; idx += 256) {
         const int k = idx >> 6, r = idx & 63;
-        Is[k][r] = inv[idx];
+        Is[k][r] = trans ? inv[r * kLeaf + k] : inv[idx];
         const int c = idx >> 6, kk = idx & 63;
         Bs[kk][c] = (kk < rows && c0 + c < cols) ? B[(c0 + c) * ldb + kk] : 0.f;
     }
@@ -216,11 +228,17 @@ hdbf_status potf2_small(hdbf_context* ctx, int n, float* A, long long lda, int* 
 hdbf_status tri_inv64(hdbf_context* ctx, int n, const float* L, long long ldl, bool unit,
                       float* out)
 {
+    return tri_inv64_mode(ctx, n, L, ldl, unit ? 1 : 0, out);
+}
+
+hdbf_status tri_inv64_mode(hdbf_context* ctx, int n, const float* L, long long ldl, int mode,
+                           float* out)
+{
     if (n <= 0) return HDBF_STATUS_SUCCESS;
     const int blocks = (n + kLeaf - 1) / kLeaf;
     ProfScope prof(ctx, kClsTrsmInv, (double)blocks * kLeaf * kLeaf * kLeaf / 3.0,
                    8.0 * blocks * kLeaf * kLeaf);
-    tri_inv64_kernel<<<blocks, kLeaf, 0, ctx->stream>>>(n, L, ldl, unit ? 1 : 0, out);
+    tri_inv64_kernel<<<blocks, kLeaf, 0, ctx->stream>>>(n, L, ldl, mode, out);
     ctx->launches++;
     return last_cuda(ctx);
 }
@@ -228,11 +246,18 @@ hdbf_status tri_inv64(hdbf_context* ctx, int n, const float* L, long long ldl, b
 hdbf_status llu_apply(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
                       long long ldb)
 {
+    return llu_apply_t(ctx, rows, cols, inv, B, ldb, false);
+}
+
+hdbf_status llu_apply_t(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
+                        long long ldb, bool trans)
+{
     if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
     if (rows > kLeaf) return HDBF_STATUS_INVALID_VALUE;
     const long long grid = ((long long)cols + kLeaf - 1) / kLeaf;
     ProfScope prof(ctx, kClsTrsmL, 2.0 * kLeaf * kLeaf * (double)cols, 8.0 * rows * cols);
-    llu_apply_kernel<<<(unsigned)grid, 256, 0, ctx->stream>>>(rows, cols, inv, B, ldb);
+    llu_apply_kernel<<<(unsigned)grid, 256, 0, ctx->stream>>>(rows, cols, inv, B, ldb,
+                                                               trans ? 1 : 0);
     ctx->launches++;
     return last_cuda(ctx);
 }

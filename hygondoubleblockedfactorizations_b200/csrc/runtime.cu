@@ -319,6 +319,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
     cudaMemset(ctx->dev_small, 0, kSmallInts * sizeof(int));
     configure_getrf_kernels(ctx);
     configure_tc_kernels(ctx);
+    configure_solve_kernels(ctx);
     const int one = 1;  // exchange epoch starts at 1: zeroed slots never match
     cudaMemcpy(ctx->dev_small + kSmallEpoch, &one, sizeof(int), cudaMemcpyHostToDevice);
     cudaDeviceSynchronize();

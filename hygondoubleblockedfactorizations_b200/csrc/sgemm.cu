@@ -1,8 +1,9 @@
-// FP32 SIMT trailing-update GEMM / SYRK:  C -= A * op(B).
+// FP32 SIMT trailing-update GEMM / SYRK:  C -= op(A) * op(B).
 //
 // Replaces the reference's rocblas_sgemm (N,T) and (N,N) update calls
 // (src/gemm/update_gemm.cpp:29-44, src/getrf/getrf_npvt_internal.h:109-124)
-// and rocblas_ssyrk lower (src/syrk/kblocked_syrk.cpp:33-45).
+// and rocblas_ssyrk lower (src/syrk/kblocked_syrk.cpp:33-45); the (T,N) form
+// serves the transposed-factor back substitution of the solves.
 //
 // Design: 128x128 CTA tile, K-step 8, 256 threads each owning an 8x8
 // register micro-tile (two 4-row x two 4-column quads, so the shared-memory
@@ -20,6 +21,10 @@ constexpr int BN = 128;
 constexpr int BK = 8;
 constexpr int NTHR = 256;
 
+// Operand forms: C -= A * B^T (NT: A is M x K, B is N x K), C -= A * B (NN: B
+// is K x N), C -= A^T * B (TN: A is K x M, B is K x N).  All column-major.
+enum Mode { kNT = 0, kNN = 1, kTN = 2 };
+
 template <bool VEC>
 __device__ __forceinline__ float4 load_col4(const float* p, int row, int rows_valid)
 {
@@ -36,40 +41,51 @@ __device__ __forceinline__ float4 load_col4(const float* p, int row, int rows_va
     return v;
 }
 
-template <bool NN, bool VEC, bool TRI>
+template <int MODE, bool VEC, bool TRI>
 __global__ void __launch_bounds__(NTHR, 2)
 sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda,
                  const float* __restrict__ B, long long ldb, float* __restrict__ C,
                  long long ldc, int tiles_m)
 {
+    constexpr bool AT = MODE == kTN;  // A read k-contiguous (transposed load)
+    constexpr bool BT = MODE != kNT;  // B read k-contiguous (transposed load)
     const int tm = blockIdx.x % tiles_m;
     const int tn = blockIdx.x / tiles_m;
     const int m0 = tm * BM;
     const int n0 = tn * BN;
     if (TRI && m0 + BM <= n0) return;  // tile strictly above the diagonal
 
-    constexpr int BSTR = NN ? BN + 4 : BN;  // pad breaks STS bank conflicts (NN)
-    __shared__ __align__(16) float As[2][BK][BM];
+    constexpr int ASTR = AT ? BM + 4 : BM;  // pad breaks STS bank conflicts
+    constexpr int BSTR = BT ? BN + 4 : BN;
+    __shared__ __align__(16) float As[2][BK][ASTR];
     __shared__ __align__(16) float Bs[2][BK][BSTR];
 
     const int tid = threadIdx.x;
-    const int ak = tid >> 5;
-    const int ar = (tid & 31) * 4;
-    const int bk = NN ? (tid & 1) * 4 : (tid >> 5);
-    const int bn = NN ? (tid >> 1) : (tid & 31) * 4;
+    // k-contiguous operands: a thread loads 4 consecutive k of one row/column
+    // (index t>>1, k offset (t&1)*4); mn-contiguous operands: 4 consecutive
+    // rows of one k column ((t&31)*4, t>>5).
+    const int ak = AT ? (tid & 1) * 4 : (tid >> 5);
+    const int am = AT ? (tid >> 1) : (tid & 31) * 4;
+    const int bk = BT ? (tid & 1) * 4 : (tid >> 5);
+    const int bn = BT ? (tid >> 1) : (tid & 31) * 4;
 
-    const float* a_ptr = A + (long long)ak * lda + (m0 + ar);
-    const float* b_ptr = NN ? B + (long long)(n0 + bn) * ldb + bk
-                            : B + (long long)bk * ldb + (n0 + bn);
-    const long long a_step = (long long)BK * lda;
-    const long long b_step = NN ? (long long)BK : (long long)BK * ldb;
+    const float* a_ptr =
+        AT ? A + (long long)(m0 + am) * lda + ak : A + (long long)ak * lda + (m0 + am);
+    const float* b_ptr =
+        BT ? B + (long long)(n0 + bn) * ldb + bk : B + (long long)bk * ldb + (n0 + bn);
+    const long long a_step = AT ? (long long)BK : (long long)BK * lda;
+    const long long b_step = BT ? (long long)BK : (long long)BK * ldb;
 
     auto fetch_a = [&](int k0) -> float4 {
-        if (k0 + ak < K) return load_col4<VEC>(a_ptr, m0 + ar, M);
+        if (AT) {
+            if (m0 + am < M) return load_col4<VEC>(a_ptr, k0 + ak, K);
+            return make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (k0 + ak < K) return load_col4<VEC>(a_ptr, m0 + am, M);
         return make_float4(0.f, 0.f, 0.f, 0.f);
     };
     auto fetch_b = [&](int k0) -> float4 {
-        if (NN) {
+        if (BT) {
             if (n0 + bn < N) return load_col4<VEC>(b_ptr, k0 + bk, K);
             return make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -77,8 +93,15 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
         return make_float4(0.f, 0.f, 0.f, 0.f);
     };
     auto stash = [&](int buf, float4 ra, float4 rb) {
-        *reinterpret_cast<float4*>(&As[buf][ak][ar]) = ra;
-        if (NN) {
+        if (AT) {
+            As[buf][ak + 0][am] = ra.x;
+            As[buf][ak + 1][am] = ra.y;
+            As[buf][ak + 2][am] = ra.z;
+            As[buf][ak + 3][am] = ra.w;
+        } else {
+            *reinterpret_cast<float4*>(&As[buf][ak][am]) = ra;
+        }
+        if (BT) {
             Bs[buf][bk + 0][bn] = rb.x;
             Bs[buf][bk + 1][bn] = rb.y;
             Bs[buf][bk + 2][bn] = rb.z;
@@ -162,25 +185,24 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-template <bool NN, bool VEC, bool TRI>
+template <int MODE, bool VEC, bool TRI>
 void launch_sub(cudaStream_t s, int M, int N, int K, const float* A, long long lda,
                 const float* B, long long ldb, float* C, long long ldc)
 {
     const int tiles_m = (M + BM - 1) / BM;
     const int tiles_n = (N + BN - 1) / BN;
     const long long grid = (long long)tiles_m * tiles_n;
-    sgemm_sub_kernel<NN, VEC, TRI><<<(unsigned)grid, NTHR, 0, s>>>(M, N, K, A, lda, B, ldb,
-                                                                  C, ldc, tiles_m);
+    sgemm_sub_kernel<MODE, VEC, TRI><<<(unsigned)grid, NTHR, 0, s>>>(M, N, K, A, lda, B, ldb,
+                                                                    C, ldc, tiles_m);
 }
 
-}  // namespace
-
-hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
-                      const float* A, long long lda, const float* B, long long ldb,
-                      float* C, long long ldc)
+hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, int N, int K,
+                         const float* A, long long lda, const float* B, long long ldb, float* C,
+                         long long ldc)
 {
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
     if (!A || !B || !C) return HDBF_STATUS_INVALID_VALUE;
+    if (lower_only && mode != kNT) return HDBF_STATUS_INVALID_VALUE;
     const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
     if (tiles > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
     const bool vec = aligned16(A) && aligned16(B) && aligned16(C) && (lda % 4 == 0) &&
@@ -194,17 +216,38 @@ hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N,
     }
     ProfScope prof(ctx, kClsGemm, flops, 4.0 * ((double)M * K + (double)N * K + 2.0 * M * N), M,
                    N, K);
-#define HDBF_SUB(NNv, VECv, TRIv) launch_sub<NNv, VECv, TRIv>(s, M, N, K, A, lda, B, ldb, C, ldc)
-    if (nn) {
-        if (vec) { if (lower_only) HDBF_SUB(true, true, true); else HDBF_SUB(true, true, false); }
-        else { if (lower_only) HDBF_SUB(true, false, true); else HDBF_SUB(true, false, false); }
+    if (mode == kNT) {
+        if (vec) {
+            if (lower_only) launch_sub<kNT, true, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
+            else launch_sub<kNT, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        } else {
+            if (lower_only) launch_sub<kNT, false, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
+            else launch_sub<kNT, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        }
+    } else if (mode == kNN) {
+        if (vec) launch_sub<kNN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        else launch_sub<kNN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
     } else {
-        if (vec) { if (lower_only) HDBF_SUB(false, true, true); else HDBF_SUB(false, true, false); }
-        else { if (lower_only) HDBF_SUB(false, false, true); else HDBF_SUB(false, false, false); }
+        if (vec) launch_sub<kTN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        else launch_sub<kTN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
     }
-#undef HDBF_SUB
     ctx->launches++;
     return last_cuda(ctx);
+}
+
+}  // namespace
+
+hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
+                      const float* A, long long lda, const float* B, long long ldb,
+                      float* C, long long ldc)
+{
+    return sgemm_launch(ctx, nn ? kNN : kNT, lower_only, M, N, K, A, lda, B, ldb, C, ldc);
+}
+
+hdbf_status sgemm_sub_tn(hdbf_context* ctx, int M, int N, int K, const float* A, long long lda,
+                         const float* B, long long ldb, float* C, long long ldc)
+{
+    return sgemm_launch(ctx, kTN, false, M, N, K, A, lda, B, ldb, C, ldc);
 }
 
 }  // namespace hdbf

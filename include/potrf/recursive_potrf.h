@@ -25,6 +25,16 @@ void recursive_potrf_tiled_trsm(hdbf_handle handle, StreamPool* pool, float* A, 
                                 int n, int nb, int* info);
 
 
+/* reference recursive_potrf.h:31-37.  Mixed-precision Cholesky: FP32 panels
+ * and FP16 tensor-core (tcgen05) trailing updates with FP32 accumulation and
+ * FP32 C (the reference rounds C to FP16, mixed_gemm.cpp:53-89), block nb.
+ * On a failed factorization it keeps the reference's damping retry: restore A,
+ * add lambda*I (lambda0 = 1e-4 * max|a_ii|, the reference's 6.55 on its
+ * 65504-scaled matrix), double lambda, at most 5 attempts
+ * (recursive_potrf.cpp:288-314, 375).  Synchronises the stream. */
+void recursive_potrf_mixed_driver(hdbf_handle handle, StreamPool* pool, float* A, int lda,
+                                  int n, int nb, int* info);
+
 #ifdef __cplusplus
 }
 #endif

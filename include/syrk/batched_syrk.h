@@ -16,6 +16,10 @@ void batched_syrk_bottom_up(hdbf_handle handle, StreamPool* pool, float* A, int 
                             float* C, int ldc, int n, int k, int nb);
 
 
+/* reference batched_syrk.h:40-43: FP16 tensor-core products, FP32 C. */
+void batched_syrk_bottom_up_mixed(hdbf_handle handle, StreamPool* pool, float* A, int lda,
+                                  float* C, int ldc, int n, int k, int nb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,6 +19,11 @@ void recursive_trsm_tiled_update(hdbf_handle handle, float* A, int lda, float* B
                                  int n, int m, int nb);
 
 
+/* reference recursive_trsm.h:35-45: update GEMMs on FP16 tensor cores with
+ * FP32 accumulation and FP32 B; FP32 leaves of order <= nb. */
+void recursive_trsm_mixed(hdbf_handle handle, float* A, int lda, float* B, int ldb, int n, int m,
+                          int nb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -310,6 +310,38 @@ def general_uniform(n: int, seed: int) -> np.ndarray:
     return uniform_pm1(n * n, seed).reshape(n, n, order="F")
 
 
+def orthogonal(n: int, seed: int) -> np.ndarray:
+    """Q from the QR factorization of an iid N(0,1) matrix (sign-fixed)."""
+    rng = np.random.default_rng(seed)
+    Q, R = np.linalg.qr(rng.standard_normal((n, n)))
+    return Q * np.sign(np.diag(R))
+
+
+def spd_kappa(n: int, kappa: float, seed: int) -> np.ndarray:
+    """FP64 SPD A = Q diag(lambda) Q^T, lambda log-spaced in [1, kappa]."""
+    Q = orthogonal(n, seed)
+    lam = np.logspace(0.0, np.log10(kappa), n)
+    A = (Q * lam) @ Q.T
+    return 0.5 * (A + A.T)
+
+
+def general_kappa(n: int, kappa: float, seed: int) -> np.ndarray:
+    """FP64 general A = U diag(sigma) V^T, sigma log-spaced in [1, kappa]."""
+    U = orthogonal(n, seed)
+    V = orthogonal(n, seed + 7919)
+    sig = np.logspace(0.0, np.log10(kappa), n)
+    return (U * sig) @ V.T
+
+
+def backward_error(A: np.ndarray, X: np.ndarray, B: np.ndarray) -> float:
+    """max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) in FP64."""
+    R = B - A @ X
+    an = np.abs(A).sum(axis=1).max()
+    num = np.abs(R).max(axis=0)
+    den = an * np.abs(X).max(axis=0) + np.abs(B).max(axis=0)
+    return float((num / den).max())
+
+
 def spd_gram(n: int, seed: int) -> np.ndarray:
     """A = G G^T / n + I formed in FP64 then rounded to FP32 (G iid U[-1,1) FP32)."""
     G = general_uniform(n, seed).astype(np.float64)
