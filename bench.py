@@ -33,6 +33,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -230,6 +232,71 @@ class Workload:
         self.getrf(self.gen, self.ipiv)
 
 
+def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
+    """Time-to-solution of A x = b to FP64 backward error <= 1e-13 (configs
+    of the mixed-precision workload): FP32 factors + FP64 refinement versus
+    tensor-core (BF16/FP16) factors + FP64 refinement, SPD and general A with
+    singular values log-spaced in [1, kappa] (Q from QR of an N(0,1) matrix)."""
+    import ctypes
+    gen = torch.Generator(device="cuda")
+    out = {}
+    mats = {}
+
+    def matrix(kind, kappa):
+        key = (kind, kappa)
+        if key in mats:
+            return mats[key]
+        mats.clear()
+        torch.cuda.empty_cache()
+        gen.manual_seed(seed)
+        Q, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen))
+        lam = torch.logspace(0.0, float(np.log10(kappa)), n, dtype=torch.float64, device="cuda")
+        if kind == "spd":
+            A = (Q * lam) @ Q.t()
+            A = 0.5 * (A + A.t())
+        else:
+            V, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen))
+            A = (Q * lam) @ V.t()
+        del Q
+        A = A.t().contiguous()  # column-major storage
+        B = torch.randn(nrhs, n, dtype=torch.float64, device="cuda", generator=gen).contiguous()
+        mats[key] = (A, B)
+        return A, B
+
+    for kind, kappa, prec in cases:
+        A, B = matrix(kind, kappa)
+        X = torch.zeros(nrhs, n, dtype=torch.float64, device="cuda")
+        fn = "hdbf_dposv_mixed" if kind == "spd" else "hdbf_dgesv_mixed"
+        res = {}
+        for p in ("fp32", prec):
+            info = hd.IrInfo()
+            args = (handle.ptr, hd.PREC[p], 1, A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
+                    X.data_ptr(), n, ctypes.c_double(1e-13), 30, ctypes.byref(info))
+            hd.call(fn, *args)  # builds the graphs and the workspace
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st = hd.call(fn, *args)
+            e1.record()
+            torch.cuda.synchronize()
+            res[p] = {"ms": round(e0.elapsed_time(e1), 2), "status": int(st),
+                      "converged": int(info.converged), "iterations": int(info.iterations),
+                      "backward_error": float(info.backward_error),
+                      "final_precision": int(info.final_precision),
+                      "factorizations": int(info.factorizations),
+                      "factor_ms": round(info.factor_ms, 2), "refine_ms": round(info.refine_ms, 2)}
+        flops = (n ** 3 / 3.0) if kind == "spd" else (2.0 * n ** 3 / 3.0)
+        r32, rm = res["fp32"], res[prec]
+        out[f"{'potrf' if kind == 'spd' else 'getrf'}_k{kappa:.0e}_{prec}"] = {
+            "fp32_ir": r32, "mixed_ir": rm,
+            "speedup_time_to_solution": round(r32["ms"] / rm["ms"], 3) if rm["ms"] > 0 else None,
+            "mixed_effective_tflops": round(flops / (rm["ms"] / 1e3) / 1e12, 2),
+            "fp32_effective_tflops": round(flops / (r32["ms"] / 1e3) / 1e12, 2)}
+    mats.clear()
+    torch.cuda.empty_cache()
+    return out
+
+
 def gpu_index():
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     if vis and vis.split(",")[0].strip().isdigit():
@@ -348,6 +415,12 @@ def run_ours(args, rank, world):
                "ms_per_step": round(e2e_ms / args.steps, 3)}
         del h_spd, h_gen, o_spd, o_gen
 
+    mixed = None
+    if not args.skip_mixed and world == 1:
+        cases = [("spd", 1e2, "bf16"), ("gen", 1e2, "bf16"), ("spd", 1e6, "fp16x3"),
+                 ("gen", 1e6, "fp16x3")]
+        mixed = mixed_ir_cases(torch, hd, handle, n, cases)
+
     total_flops = world * args.steps * (flops_potrf(n) + flops_getrf(n))
     value = total_flops / (ms_max / 1e3) / 1e12
 
@@ -385,7 +458,7 @@ def run_ours(args, rank, world):
            "potrf_tflops": round(flops_potrf(n) / (ms_potrf / 1e3) / 1e12, 3),
            "getrf_tflops": round(flops_getrf(n) / (ms_getrf / 1e3) / 1e12, 3),
            "info": info, "gpu_launches": launches, "kernels": kernels,
-           "roofline": roof, "clocks": clocks, "e2e": e2e}
+           "roofline": roof, "clocks": clocks, "e2e": e2e, "mixed_ir": mixed}
     return out, handle
 
 
@@ -398,6 +471,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-mixed", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

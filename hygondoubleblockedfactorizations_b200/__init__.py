@@ -87,6 +87,8 @@ _PROTOS = {
                                  c_double, c_int, P]),
     "hdbf_dgesv_mixed": (c_int, [P, c_int, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
                                  c_double, c_int, P]),
+    "hdbf_batched_num_variants": (c_int, []),
+    "hdbf_batched_factor_solve": (c_int, [P, c_int, c_int, P, P, P, P, P, P, P, P, P]),
     "launch_mixed_gemm": (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_float, P, c_int, P,
                                  c_int, c_float, P, c_int]),
     # kernels

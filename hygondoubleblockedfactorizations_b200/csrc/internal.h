@@ -119,8 +119,9 @@ void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st);
 //   inv   inverted 64x64 diagonal blocks, n*64 floats
 //   src, tgt, gperm  composed row moves / permutation scratch, n ints each
 //   temp  column-tiled swap buffer, 64*n floats
+//   skinny  split-K partial sums of the skinny GEMM, 256*n floats
 struct WsLayout {
-    size_t coop, inv, src, tgt, gperm, temp, total;
+    size_t coop, inv, src, tgt, gperm, temp, skinny, total;
 };
 WsLayout ws_layout(int n);
 // Guarantee the layout for order n (grows the arena outside stream capture).
@@ -131,6 +132,7 @@ int* ws_src(hdbf_context* ctx);
 int* ws_tgt(hdbf_context* ctx);
 int* ws_gperm(hdbf_context* ctx);
 float* ws_temp(hdbf_context* ctx);
+float* ws_skinny(hdbf_context* ctx);
 
 hdbf_status last_cuda(hdbf_context* ctx);
 
@@ -143,6 +145,13 @@ hdbf_status last_cuda(hdbf_context* ctx);
 hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
                       const float* A, long long lda, const float* B, long long ldb,
                       float* C, long long ldc);
+
+// Skinny update (N <= 32): mode 0 C -= A * B^T, 1 C -= A * B, 2 C -= A^T * B,
+// with the operand shapes of sgemm_sub / sgemm_sub_tn.  sgemm_launch routes
+// narrow non-triangular updates here.
+hdbf_status sgemm_skinny(hdbf_context* ctx, int mode, int M, int N, int K, const float* A,
+                         long long lda, const float* B, long long ldb, float* C, long long ldc);
+size_t skinny_partial_floats(int n);
 
 // C(M x N) -= A^T * B with A stored K x M and B stored K x N (column-major).
 hdbf_status sgemm_sub_tn(hdbf_context* ctx, int M, int N, int K, const float* A, long long lda,
@@ -179,6 +188,7 @@ hdbf_status potrs_f32(hdbf_context* ctx, const float* L, long long ldl, int n, i
 hdbf_status getrs_f32_permuted(hdbf_context* ctx, const float* LU, long long ldlu, int n, int nrhs,
                                float* B, long long ldb);
 void configure_solve_kernels(hdbf_context* ctx);
+void configure_batched_kernels(hdbf_context* ctx);
 
 // Cooperative partially pivoted LU of an m x w panel (w <= 32).  Pivots are
 // written 1-based as (local row + 1 + ipiv_add).

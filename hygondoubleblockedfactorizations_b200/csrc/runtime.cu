@@ -96,6 +96,8 @@ WsLayout ws_layout(int n)
     off += align_up((size_t)n * sizeof(int), 256);
     L.temp = off;
     off += align_up((size_t)64 * n * sizeof(float), 256);
+    L.skinny = off;
+    off += align_up(skinny_partial_floats(n) * sizeof(float), 256);
     L.total = off;
     return L;
 }
@@ -143,6 +145,10 @@ int* ws_gperm(hdbf_context* ctx)
 float* ws_temp(hdbf_context* ctx)
 {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).temp);
+}
+float* ws_skinny(hdbf_context* ctx)
+{
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).skinny);
 }
 
 ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes, int m, int n,
@@ -320,6 +326,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
     configure_getrf_kernels(ctx);
     configure_tc_kernels(ctx);
     configure_solve_kernels(ctx);
+    configure_batched_kernels(ctx);
     const int one = 1;  // exchange epoch starts at 1: zeroed slots never match
     cudaMemcpy(ctx->dev_small + kSmallEpoch, &one, sizeof(int), cudaMemcpyHostToDevice);
     cudaDeviceSynchronize();

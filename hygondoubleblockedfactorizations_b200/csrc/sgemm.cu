@@ -153,10 +153,36 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
         buf ^= 1;
     }
 
-    // Epilogue: C -= acc.
+    // Epilogue: C -= acc.  Full interior tiles read all 16 C quads before
+    // writing any (independent loads in flight together).
     const bool full_rows = (m0 + BM <= M);
     const bool full_cols = (n0 + BN <= N);
     const bool below_diag = !TRI || (m0 >= n0 + BN);
+    if (VEC && full_rows && full_cols && below_diag) {
+        float4 cq[8][2];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                cq[j][h] = __ldcg(reinterpret_cast<const float4*>(C + (long long)col * ldc + m0 +
+                                                                  h * 64 + ty * 4));
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float4 c = cq[j][h];
+                c.x -= acc[h * 4 + 0][j];
+                c.y -= acc[h * 4 + 1][j];
+                c.z -= acc[h * 4 + 2][j];
+                c.w -= acc[h * 4 + 3][j];
+                *reinterpret_cast<float4*>(C + (long long)col * ldc + m0 + h * 64 + ty * 4) = c;
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
@@ -165,14 +191,7 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int row = m0 + h * 64 + ty * 4;
-            if (VEC && full_rows && full_cols && below_diag) {
-                float4 c = *reinterpret_cast<float4*>(cp + row);
-                c.x -= acc[h * 4 + 0][j];
-                c.y -= acc[h * 4 + 1][j];
-                c.z -= acc[h * 4 + 2][j];
-                c.w -= acc[h * 4 + 3][j];
-                *reinterpret_cast<float4*>(cp + row) = c;
-            } else {
+            {
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int r = row + i;
@@ -203,6 +222,9 @@ hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, in
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
     if (!A || !B || !C) return HDBF_STATUS_INVALID_VALUE;
     if (lower_only && mode != kNT) return HDBF_STATUS_INVALID_VALUE;
+    if (!lower_only && N <= 32 && M >= 4 * N && M >= 256)
+        return sgemm_skinny(ctx, mode == kNT ? 0 : mode == kNN ? 1 : 2, M, N, K, A, lda, B, ldb,
+                            C, ldc);
     const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
     if (tiles > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
     const bool vec = aligned16(A) && aligned16(B) && aligned16(C) && (lda % 4 == 0) &&

@@ -210,15 +210,32 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
             : "memory");
     }
 
+    // Prefetch this thread's first 32 C values while the MMAs drain.
+    const int row = m0 + warp * 32 + lane;
+    float cv[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const int col = n0 + j;
+        cv[j] = (row < args.M && col < args.N) ? __ldcg(args.C + (long long)col * args.ldc + row)
+                                               : 0.f;
+    }
     __syncwarp();
     const bool ok = mbar_wait(&done_bar, 0, args.err);
     asm volatile("tcgen05.fence::after_thread_sync;");
     __syncthreads();
     if (ok && !s_fail && ktiles > 0) {
-        const int row = m0 + warp * 32 + lane;
         const uint32_t lane_base = taddr + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
         for (int c0 = 0; c0 < TN; c0 += 32) {
+            if (c0 > 0) {  // all 32 loads of the chunk in flight together
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = n0 + c0 + j;
+                    cv[j] = (row < args.M && col < args.N)
+                                ? __ldcg(args.C + (long long)col * args.ldc + row)
+                                : 0.f;
+                }
+            }
             uint32_t v[32];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -236,10 +253,9 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int col = n0 + c0 + j;
-                    if (col < args.N && (!args.lower || row >= col)) {
-                        float* cp = args.C + (long long)col * args.ldc + row;
-                        *cp = fmaf(-args.scale, __uint_as_float(v[j]), *cp);
-                    }
+                    if (col < args.N && (!args.lower || row >= col))
+                        args.C[(long long)col * args.ldc + row] =
+                            fmaf(-args.scale, __uint_as_float(v[j]), cv[j]);
                 }
             }
         }

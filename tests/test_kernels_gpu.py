@@ -44,6 +44,24 @@ def test_gemm_nt_update(hd, handle, torch_cuda, M, N, K, pad):
         assert np.all(np.isnan(got[M:]))
 
 
+@pytest.mark.parametrize("M,N,K", [(256, 1, 1), (300, 8, 33), (4096, 16, 1024), (5000, 31, 4099),
+                                   (70000, 32, 96), (1024, 9, 20000)])
+def test_gemm_nt_update_skinny(hd, handle, torch_cuda, M, N, K):
+    # narrow updates take the row-per-thread kernel; with the workspace
+    # reserved, long K is split across CTAs and reduced in a fixed order
+    handle.reserve(256 << 20)
+    A, B, C = rnd((M, K), 11), rnd((N, K), 12), rnd((M, N), 13)
+    lda, ldb, ldc = M + 3, N + 1, M + 5
+    dA, dB, dC = put(torch_cuda, A, lda), put(torch_cuda, B, ldb), put(torch_cuda, C, ldc)
+    hd.call("gemm_nt_update", handle.ptr, M, N, K, ptr(dA), lda, ptr(dB), ldb, ptr(dC), ldc)
+    torch_cuda.cuda.synchronize()
+    handle.check()
+    got = host2d(dC, ldc, ldc, N)
+    want = C.astype(np.float64) - A.astype(np.float64) @ B.astype(np.float64).T
+    assert rel_err(got[:M], want) <= tol(K)
+    assert np.all(np.isnan(got[M:]))
+
+
 def test_gemm_nt_update_m_tiled(hd, handle, torch_cuda):
     M, N, K = 1000, 200, 96
     A, B, C = rnd((M, K), 4), rnd((N, K), 5), rnd((M, N), 6)
