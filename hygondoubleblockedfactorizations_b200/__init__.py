@@ -43,6 +43,7 @@ _PROTOS = {
     "hdbf_profile_class_name": (ctypes.c_char_p, [c_int]),
     "hdbf_profile_num_classes": (c_int, []),
     "hdbf_set_graph_mode": (c_int, [P, c_int]),
+    "hdbf_set_panel_kernel": (c_int, [P, c_int]),
     # potrf
     "double_blocked_potrf": (None, [P, P, c_int, c_int, c_int, c_int, P]),
     "double_blocked_potrf_dbtrsm": (None, [P, P, c_int, c_int, c_int, c_int, P]),
@@ -87,6 +88,11 @@ _PROTOS = {
                                  c_double, c_int, P]),
     "hdbf_dgesv_mixed": (c_int, [P, c_int, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
                                  c_double, c_int, P]),
+    "hdbf_selector_num_params": (c_int, [c_int, c_int]),
+    "hdbf_selector_init": (c_int, [P, P, c_int, c_int, c_ull]),
+    "hdbf_selector_train": (c_int, [P, P, P, P, c_int, P, P, P, c_int, c_int, c_int, c_int,
+                                    c_float, c_float, P, P]),
+    "hdbf_selector_predict": (c_int, [P, P, P, P, c_int, c_int, c_int, P, P, P]),
     "hdbf_batched_num_variants": (c_int, []),
     "hdbf_batched_factor_solve": (c_int, [P, c_int, c_int, P, P, P, P, P, P, P, P, P]),
     "launch_mixed_gemm": (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_float, P, c_int, P,
@@ -178,6 +184,12 @@ class Handle:
         st = lib().hdbf_reserve_workspace(self._h, nbytes)
         if st != 0:
             raise HdbfError(f"reserve_workspace: {status_string(st)}")
+
+    def set_panel_kernel(self, mode: int):
+        """0 automatic, 1 grid-wide publish-and-poll kernel, 2 cluster kernel."""
+        st = lib().hdbf_set_panel_kernel(self._h, int(mode))
+        if st != 0:
+            raise HdbfError(f"set_panel_kernel: {status_string(st)}")
 
     def set_graphs(self, enabled: bool):
         lib().hdbf_set_graph_mode(self._h, 1 if enabled else 0)

@@ -438,7 +438,7 @@ hdbf_status hdbf_batched_factor_solve(hdbf_handle h, int variant, int count, con
     const int ctas = h->sm_count;  // one persistent CTA per SM (shared memory bound)
     return h->last_status = run_graph(h, key, [&]() -> hdbf_status {
         cudaMemsetAsync(queue, 0, sizeof(unsigned int), h->stream);
-        ProfScope prof(h, kClsOther, 0.0, 0.0);
+        ProfScope prof(h, kClsBatched, 0.0, 0.0);
         if (variant == 0) return launch_batched<128>(h, a, ctas);
         if (variant == 1) return launch_batched<256>(h, a, ctas);
         return launch_batched<512>(h, a, ctas);

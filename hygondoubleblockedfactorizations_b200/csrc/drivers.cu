@@ -115,7 +115,14 @@ hdbf_status getrf_panel(hdbf_context* ctx, int m, int w, float* A, long long lda
                         int ipiv_add, int* info, int info_base, bool pivot, const GetrfWs& ws)
 {
     if (m <= 0 || w <= 0) return HDBF_STATUS_SUCCESS;
-    if (w <= kPanelLeaf) return getf2_coop(ctx, m, w, A, lda, ipiv, ipiv_add, info, info_base, pivot);
+    if (w <= kPanelLeaf) {
+        if (ctx->panel_mode != 1) {
+            const hdbf_status st =
+                getf2_cluster(ctx, m, w, A, lda, ipiv, ipiv_add, info, info_base, pivot);
+            if (st != HDBF_STATUS_NOT_SUPPORTED) return st;
+        }
+        return getf2_coop(ctx, m, w, A, lda, ipiv, ipiv_add, info, info_base, pivot);
+    }
     const int w1 = split_at(w, kPanelLeaf);
     const int w2 = w - w1;
     HDBF_TRY(getrf_panel(ctx, m, w1, A, lda, ipiv, ipiv_add, info, info_base, pivot, ws));

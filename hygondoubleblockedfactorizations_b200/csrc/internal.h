@@ -13,9 +13,9 @@ namespace hdbf {
 enum KernelClass {
     kClsGemm = 0,     // sgemm_sub_kernel (GEMM / SYRK trailing updates)
     kClsPotf2 = 1,    // potf2_kernel
-    kClsTrsmR = 2,    // trsm_rlt_kernel
-    kClsTrsmL = 3,    // trsm_llu_kernel
-    kClsPanel = 4,    // getf2_coop_kernel
+    kClsTrsmR = 2,    // rlt_apply_kernel
+    kClsTrsmL = 3,    // llu_apply_kernel
+    kClsPanel = 4,    // getf2_cluster_kernel / getf2_coop_kernel
     kClsCompose = 5,  // compose_swaps_kernel
     kClsMoves = 6,    // apply_moves kernels
     kClsTrsmInv = 7,  // tri_inv64_kernel
@@ -23,7 +23,11 @@ enum KernelClass {
     kClsConvert = 9,  // FP32 -> 16-bit shadow conversions
     kClsIr = 10,      // FP64 residual / update / norm kernels
     kClsOther = 11,
-    kNumClasses = 12
+    kClsWave = 12,     // trsv_wave_kernel (wavefront triangular solves)
+    kClsSkinny = 13,   // skinny_kernel (updates with N <= 32)
+    kClsBatched = 14,  // batched_factor_solve_kernel
+    kClsSelector = 15, // selector MLP kernels
+    kNumClasses = 16
 };
 struct ProfRec {
     int cls;
@@ -47,6 +51,8 @@ struct hdbf_context {
     int device = 0;
     int sm_count = 148;
     size_t max_smem_optin = 0;
+    int cluster_max = 0;  // largest cluster the panel kernel can launch (0: none)
+    int panel_mode = 0;   // hdbf_set_panel_kernel
     // Workspace arena (grown on demand outside stream capture).
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -116,12 +122,13 @@ void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st);
 
 // Workspace layout for problems of order <= n (byte offsets):
 //   coop  panel-kernel exchange slots (fixed size, offset 0)
-//   inv   inverted 64x64 diagonal blocks, n*64 floats
+//   inv   inverted 64x64 diagonal blocks, ceil(n/64)*4096 floats
 //   src, tgt, gperm  composed row moves / permutation scratch, n ints each
 //   temp  column-tiled swap buffer, 64*n floats
 //   skinny  split-K partial sums of the skinny GEMM, 256*n floats
+//   wave  wavefront-solve row-major x copy (32 columns) and its flags
 struct WsLayout {
-    size_t coop, inv, src, tgt, gperm, temp, skinny, total;
+    size_t coop, inv, src, tgt, gperm, temp, skinny, wave, total;
 };
 WsLayout ws_layout(int n);
 // Guarantee the layout for order n (grows the arena outside stream capture).
@@ -133,6 +140,7 @@ int* ws_tgt(hdbf_context* ctx);
 int* ws_gperm(hdbf_context* ctx);
 float* ws_temp(hdbf_context* ctx);
 float* ws_skinny(hdbf_context* ctx);
+float* ws_wave(hdbf_context* ctx);
 
 hdbf_status last_cuda(hdbf_context* ctx);
 
@@ -188,6 +196,16 @@ hdbf_status potrs_f32(hdbf_context* ctx, const float* L, long long ldl, int n, i
 hdbf_status getrs_f32_permuted(hdbf_context* ctx, const float* LU, long long ldlu, int n, int nrhs,
                                float* B, long long ldb);
 void configure_solve_kernels(hdbf_context* ctx);
+
+// Wavefront block triangular solve (trsm_wave.cu): B <- op(M)^{-1} B, M = T
+// (trans false) or T^T (trans true); forward for a lower M, backward for an
+// upper one.  inv holds the 64x64 diagonal-block inverses of T from
+// tri_inv64_mode (applied transposed when trans is set).  One launch per 32
+// right-hand-side columns.
+hdbf_status trsv_wave(hdbf_context* ctx, int n, int nrhs, const float* T, long long ldt, bool trans,
+                      const float* inv, bool backward, float* B, long long ldb);
+size_t wave_scratch_bytes(int n);
+void configure_wave_kernels(hdbf_context* ctx);
 void configure_batched_kernels(hdbf_context* ctx);
 
 // Cooperative partially pivoted LU of an m x w panel (w <= 32).  Pivots are
@@ -196,6 +214,12 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
                        int ipiv_add, int* info, int info_base, bool pivot);
 size_t getf2_coop_scratch_bytes();
 void configure_getrf_kernels(hdbf_context* ctx);
+// Same contract on one thread-block cluster with the block in distributed
+// shared memory; NOT_SUPPORTED when the block does not fit (caller falls
+// back to getf2_coop).
+hdbf_status getf2_cluster(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
+                          int ipiv_add, int* info, int info_base, bool pivot);
+int configure_cluster_panel(hdbf_context* ctx);
 
 // Compose LAPACK swaps  row (i) <-> row (ipiv[i]-1-ipiv_minus), i in [0,k),
 // over local rows [0, m) into (src, tgt, *count) moves.

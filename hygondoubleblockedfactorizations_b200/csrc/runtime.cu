@@ -86,8 +86,8 @@ WsLayout ws_layout(int n)
     size_t off = 0;
     L.coop = off;
     off += getf2_coop_scratch_bytes();
-    L.inv = off;
-    off += align_up((size_t)n * 64 * sizeof(float), 256);
+    L.inv = off;  // whole 64x64 blocks, the last one padded
+    off += align_up((size_t)(n + 63) / 64 * 64 * 64 * sizeof(float), 256);
     L.src = off;
     off += align_up((size_t)n * sizeof(int), 256);
     L.tgt = off;
@@ -98,6 +98,8 @@ WsLayout ws_layout(int n)
     off += align_up((size_t)64 * n * sizeof(float), 256);
     L.skinny = off;
     off += align_up(skinny_partial_floats(n) * sizeof(float), 256);
+    L.wave = off;
+    off += wave_scratch_bytes(n);
     L.total = off;
     return L;
 }
@@ -145,6 +147,10 @@ int* ws_gperm(hdbf_context* ctx)
 float* ws_temp(hdbf_context* ctx)
 {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).temp);
+}
+float* ws_wave(hdbf_context* ctx)
+{
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).wave);
 }
 float* ws_skinny(hdbf_context* ctx)
 {
@@ -324,6 +330,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
     }
     cudaMemset(ctx->dev_small, 0, kSmallInts * sizeof(int));
     configure_getrf_kernels(ctx);
+    ctx->cluster_max = configure_cluster_panel(ctx);
     configure_tc_kernels(ctx);
     configure_solve_kernels(ctx);
     configure_batched_kernels(ctx);
@@ -532,14 +539,26 @@ const char* hdbf_profile_class_name(int cls)
 {
     static const char* names[kNumClasses] = {"sgemm_sub_kernel", "potf2_kernel",
                                              "rlt_apply_kernel", "llu_apply_kernel",
-                                             "getf2_coop_kernel", "compose_swaps_kernel",
+                                             "getf2_panel_kernel", "compose_swaps_kernel",
                                              "apply_moves", "tri_inv64_kernel",
                                              "tc_gemm_sub_kernel", "convert16_kernels",
-                                             "ir_fp64_kernels", "other"};
+                                             "ir_fp64_kernels", "other",
+                                             "trsv_wave_kernel", "sgemm_skinny_kernel",
+                                             "batched_factor_solve_kernel",
+                                             "selector_mlp_kernels"};
     return (cls >= 0 && cls < kNumClasses) ? names[cls] : "unknown";
 }
 
 int hdbf_profile_num_classes(void) { return kNumClasses; }
+
+hdbf_status hdbf_set_panel_kernel(hdbf_handle h, int mode)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    if (mode < 0 || mode > 2) return HDBF_STATUS_INVALID_VALUE;
+    if (mode != h->panel_mode) graph_cache_clear(h);
+    h->panel_mode = mode;
+    return HDBF_STATUS_SUCCESS;
+}
 
 hdbf_status hdbf_set_graph_mode(hdbf_handle h, int enabled)
 {

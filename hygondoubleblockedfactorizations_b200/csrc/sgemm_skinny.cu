@@ -108,7 +108,7 @@ hdbf_status sgemm_skinny(hdbf_context* ctx, int mode, int M, int N, int K, const
         else S = 1;
     }
     const int kper = (K + S - 1) / S;
-    ProfScope prof(ctx, kClsGemm, 2.0 * (double)M * N * K, 4.0 * ((double)M * K + 2.0 * M * N), M,
+    ProfScope prof(ctx, kClsSkinny, 2.0 * (double)M * N * K, 4.0 * ((double)M * K + 2.0 * M * N), M,
                    N, K);
     dim3 grid(gx, S);
     cudaStream_t st = ctx->stream;

@@ -1,8 +1,9 @@
 // Triangular solves with several right-hand sides (POTRS / GETRS) on the
 // FP32 factors.  Not part of the reference (it has no solve); needed by the
-// iterative-refinement driver.  Same scheme as the factorization TRSMs: the
-// 64x64 diagonal blocks of the triangle are inverted once per solve, the
-// recursion on row halves updates with GEMMs, leaves apply the inverses.
+// iterative-refinement driver.  The 64x64 diagonal blocks of the triangle are
+// inverted once per solve.  Up to kWaveMaxRhs right-hand sides, each
+// triangle is one wavefront launch (trsm_wave.cu); wider right-hand sides use
+// the recursion on row halves with GEMM updates and inverse leaves.
 #include <algorithm>
 
 #include "internal.h"
@@ -11,6 +12,7 @@ namespace hdbf {
 namespace {
 
 constexpr int kLeaf = 64;
+constexpr int kWaveMaxRhs = 64;
 
 inline int split_at(int n)
 {
@@ -66,14 +68,25 @@ __global__ void __launch_bounds__(1024) ipiv_to_perm_kernel(const int* ipiv, int
     int* p = use_smem ? sp : perm;
     for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = i;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < n; ++i) {
-            const int b = ipiv[i] - 1;
-            if (b != i && b >= 0 && b < n) {
-                const int t = p[i];
-                p[i] = p[b];
-                p[b] = t;
+    // The swaps are a dependent chain; warp 0 loads the next 32 pivots
+    // while lane 0 applies the current 32 (pivots arrive by shuffle).
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int cur = lane < n ? ipiv[lane] : 0;
+        for (int i0 = 0; i0 < n; i0 += 32) {
+            const int nx = i0 + 32 + lane < n ? ipiv[i0 + 32 + lane] : 0;
+            const int cnt = n - i0 < 32 ? n - i0 : 32;
+            for (int u = 0; u < cnt; ++u) {
+                const int b = __shfl_sync(0xffffffffu, cur, u) - 1;
+                const int i = i0 + u;
+                if (lane == 0 && b != i && b >= 0 && b < n) {
+                    const int t = p[i];
+                    p[i] = p[b];
+                    p[b] = t;
+                }
+                __syncwarp();
             }
+            cur = nx;
         }
     }
     __syncthreads();
@@ -121,6 +134,7 @@ void configure_solve_kernels(hdbf_context* ctx)
     cudaFuncSetAttribute(ipiv_to_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)cap);
     cudaGetLastError();
+    configure_wave_kernels(ctx);
 }
 
 // B <- L^{-T} L^{-1} B for the Cholesky factor L (lower, non-unit).
@@ -131,6 +145,10 @@ hdbf_status potrs_f32(hdbf_context* ctx, const float* L, long long ldl, int n, i
     HDBF_TRY(ensure_ws(ctx, n));
     float* inv = ws_inv(ctx);
     HDBF_TRY(tri_inv64_mode(ctx, n, L, ldl, 0, inv));
+    if (nrhs <= kWaveMaxRhs) {
+        HDBF_TRY(trsv_wave(ctx, n, nrhs, L, ldl, false, inv, false, B, ldb));
+        return trsv_wave(ctx, n, nrhs, L, ldl, true, inv, true, B, ldb);
+    }
     HDBF_TRY(fwd_lower(ctx, n, nrhs, L, ldl, B, ldb, inv));
     return bwd_lower_t(ctx, n, nrhs, L, ldl, B, ldb, inv);
 }
@@ -143,9 +161,12 @@ hdbf_status getrs_f32_permuted(hdbf_context* ctx, const float* LU, long long ldl
     if (n <= 0 || nrhs <= 0) return HDBF_STATUS_SUCCESS;
     HDBF_TRY(ensure_ws(ctx, n));
     float* inv = ws_inv(ctx);
+    const bool wave = nrhs <= kWaveMaxRhs;
     HDBF_TRY(tri_inv64_mode(ctx, n, LU, ldlu, 1, inv));
-    HDBF_TRY(fwd_lower(ctx, n, nrhs, LU, ldlu, B, ldb, inv));
+    if (wave) HDBF_TRY(trsv_wave(ctx, n, nrhs, LU, ldlu, false, inv, false, B, ldb));
+    else HDBF_TRY(fwd_lower(ctx, n, nrhs, LU, ldlu, B, ldb, inv));
     HDBF_TRY(tri_inv64_mode(ctx, n, LU, ldlu, 2, inv));
+    if (wave) return trsv_wave(ctx, n, nrhs, LU, ldlu, false, inv, true, B, ldb);
     return bwd_upper(ctx, n, nrhs, LU, ldlu, B, ldb, inv);
 }
 

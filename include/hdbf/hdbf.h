@@ -85,6 +85,13 @@ unsigned long long hdbf_launch_count(hdbf_handle handle);
  * stream are recorded into the caller's graph instead. */
 hdbf_status hdbf_set_graph_mode(hdbf_handle handle, int enabled);
 
+/* GETRF panel-leaf kernel: 0 = automatic (thread-block cluster when the
+ * column block fits in one cluster's shared memory, otherwise the
+ * grid-wide publish-and-poll kernel), 1 = always the grid-wide kernel,
+ * 2 = cluster only (blocks that do not fit still take the grid-wide kernel).
+ * Both produce identical pivots and factors. */
+hdbf_status hdbf_set_panel_kernel(hdbf_handle handle, int mode);
+
 /* Per-launch event profiling of this library's kernels on the handle's
  * stream.  Between begin and end every launch is bracketed by CUDA events;
  * end synchronises the stream and returns, per kernel class (see

@@ -63,8 +63,11 @@ def make_ws(torch, n, tile=64):
     return ws, keep
 
 
+@pytest.mark.parametrize("panel", [0, 1])
 @pytest.mark.parametrize("n,outer,inner", [(512, 256, 64), (1024, 512, 128), (2048, 1024, 256)])
-def test_pivots_identical_to_lapack_immediate(hd, handle, torch_cuda, n, outer, inner):
+def test_pivots_identical_to_lapack_immediate(hd, handle, torch_cuda, n, outer, inner, panel):
+    # panel 0: cluster panel kernel (these blocks fit), 1: grid-wide kernel
+    handle.set_panel_kernel(panel)
     G = oracle.general_uniform(n, 1)
     _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf", outer=outer,
                                   inner=inner)
@@ -79,9 +82,11 @@ def test_pivots_identical_to_lapack_immediate(hd, handle, torch_cuda, n, outer, 
     assert getrf_check(LU[:n], G, ipiv) <= BOUND
 
 
+@pytest.mark.parametrize("panel", [0, 1])
 @pytest.mark.parametrize("mode", [0, 1])
-def test_batched_pivot_variant(hd, handle, torch_cuda, mode):
+def test_batched_pivot_variant(hd, handle, torch_cuda, mode, panel):
     import ctypes
+    handle.set_panel_kernel(panel)
     n = 2048
     G = oracle.general_uniform(n, 1)
     ws, keep = make_ws(torch_cuda, n, tile=48)

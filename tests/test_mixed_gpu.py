@@ -13,7 +13,7 @@ import pytest
 
 import hygondoubleblockedfactorizations_b200 as hd_mod
 import oracle
-from tests.common import dev, host2d, info_tensor, ptr
+from tests.common import dev, host2d, info_tensor, padded, ptr
 
 pytestmark = pytest.mark.gpu
 
@@ -56,27 +56,39 @@ def test_sgetrf_mixed(hd, handle, torch_cuda, prec):
     assert r <= max(growth_tol, 16 * n * 2.0 ** -23), (prec, r)
 
 
-def test_spotrs_sgetrs(hd, handle, torch_cuda):
-    n, nrhs = 700, 16
+# nrhs <= 64 takes the wavefront solve (one launch per triangle and 32
+# columns), wider right-hand sides the recursive GEMM solve; odd leading
+# dimensions take the 4-byte tile copies, partial last blocks the zero fill.
+@pytest.mark.parametrize("n,nrhs,pad", [(700, 16, 0), (64, 1, 0), (65, 3, 1), (1000, 33, 3),
+                                        (2049, 64, 0), (513, 80, 1), (4096, 8, 0)])
+def test_spotrs_sgetrs(hd, handle, torch_cuda, n, nrhs, pad):
+    ld = n + pad
     A = oracle.spd_gram(n, 2)
     L = np.linalg.cholesky(A.astype(np.float64)).astype(np.float32)
     B = np.random.default_rng(3).standard_normal((n, nrhs)).astype(np.float32)
-    dL, dB = dev(torch_cuda, L), dev(torch_cuda, B)
-    st = hd.call("hdbf_spotrs", handle.ptr, ptr(dL), n, n, nrhs, ptr(dB), n)
+    dL, _ = padded(torch_cuda, L, ld)
+    dB, _ = padded(torch_cuda, B, ld)
+    st = hd.call("hdbf_spotrs", handle.ptr, ptr(dL), ld, n, nrhs, ptr(dB), ld)
     torch_cuda.cuda.synchronize()
-    assert st == 0
-    X = host2d(dB, n, n, nrhs)
+    assert st == 0 and handle.device_errors() == 0
+    X = host2d(dB, ld, ld, nrhs)
     want = np.linalg.solve(L.astype(np.float64) @ L.astype(np.float64).T, B.astype(np.float64))
-    assert np.abs(X - want).max() <= 1e-4 * np.abs(want).max()
+    assert np.abs(X[:n] - want).max() <= 1e-4 * np.abs(want).max()
+    if pad:
+        assert np.all(np.isnan(X[n:]))
     G = oracle.general_uniform(n, 4) + np.float32(2.0) * np.eye(n, dtype=np.float32)
     lu, piv, info = oracle.lapack_sgetrf(G)
-    dLU, dP, dB = dev(torch_cuda, lu), dev(torch_cuda, piv), dev(torch_cuda, B)
-    st = hd.call("hdbf_sgetrs", handle.ptr, ptr(dLU), n, n, ptr(dP), nrhs, ptr(dB), n)
+    dLU, _ = padded(torch_cuda, lu, ld)
+    dP = dev(torch_cuda, piv)
+    dB, _ = padded(torch_cuda, B, ld)
+    st = hd.call("hdbf_sgetrs", handle.ptr, ptr(dLU), ld, n, ptr(dP), nrhs, ptr(dB), ld)
     torch_cuda.cuda.synchronize()
-    assert st == 0
-    X = host2d(dB, n, n, nrhs)
+    assert st == 0 and handle.device_errors() == 0
+    X = host2d(dB, ld, ld, nrhs)
     want = np.linalg.solve(G.astype(np.float64), B.astype(np.float64))
-    assert np.abs(X - want).max() <= 1e-3 * np.abs(want).max()
+    assert np.abs(X[:n] - want).max() <= 1e-3 * np.abs(want).max()
+    if pad:
+        assert np.all(np.isnan(X[n:]))
 
 
 def run_ir(hd, handle, torch, fn, A, B, prec, escalate=1, tol=1e-13, max_iter=30):
