@@ -52,6 +52,35 @@ __device__ __forceinline__ bool better(float v, int i, float bv, int bi)
     return v > bv || (v == bv && i < bi);
 }
 
+// Copy an nr x w column block between global memory and the shared tile
+// (leading dimension ldt), eight independent loads in flight per thread.
+template <bool TO_SMEM>
+__device__ __forceinline__ void coop_move(float* A, long long lda, float* tile, int ldt, int nr,
+                                          int w)
+{
+    const int total = nr * w;
+    int e = threadIdx.x;
+    for (; e + 7 * kCoopThreads < total; e += 8 * kCoopThreads) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = e + u * kCoopThreads, c = q / nr, r = q - c * nr;
+            v[u] = TO_SMEM ? A[(long long)c * lda + r] : tile[c * ldt + r];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = e + u * kCoopThreads, c = q / nr, r = q - c * nr;
+            if (TO_SMEM) tile[c * ldt + r] = v[u];
+            else A[(long long)c * lda + r] = v[u];
+        }
+    }
+    for (; e < total; e += kCoopThreads) {
+        const int c = e / nr, r = e - c * nr;
+        if (TO_SMEM) tile[c * ldt + r] = A[(long long)c * lda + r];
+        else A[(long long)c * lda + r] = tile[c * ldt + r];
+    }
+}
+
 // Exchange protocol (no grid barrier): for column j every CTA writes its slot
 // (parity j&1) -- candidate |max|, its row index and that row's w values, plus
 // the diagonal row j if it owns it -- then publishes seq = epoch*64 + j + 1
@@ -84,9 +113,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     const int nr = max(0, min(m, r0 + rpc) - r0);
     const unsigned epoch = *reinterpret_cast<volatile unsigned*>(epoch_ptr);
 
-    for (int c = 0; c < w; ++c)
-        for (int r = tid; r < nr; r += kCoopThreads)
-            tile[c * rpc + r] = A[(long long)c * lda + (r0 + r)];
+    coop_move<true>(A + r0, lda, tile, rpc, nr, w);
     if (tid == 0) s_abort = 0;
     __syncthreads();
 
@@ -215,9 +242,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         __syncthreads();
     }
 
-    for (int c = 0; c < w; ++c)
-        for (int r = tid; r < nr; r += kCoopThreads)
-            A[(long long)c * lda + (r0 + r)] = tile[c * rpc + r];
+    coop_move<false>(A + r0, lda, tile, rpc, nr, w);
 
     // Advance the epoch once every CTA is done (the kernel's last action).
     __syncthreads();

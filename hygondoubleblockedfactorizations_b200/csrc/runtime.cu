@@ -331,6 +331,10 @@ hdbf_status hdbf_create(hdbf_handle* handle)
     cudaMemset(ctx->dev_small, 0, kSmallInts * sizeof(int));
     configure_getrf_kernels(ctx);
     ctx->cluster_max = configure_cluster_panel(ctx);
+    if (const char* pk = std::getenv("HDBF_PANEL_KERNEL")) {  // default panel kernel
+        const int v = std::atoi(pk);
+        if (v >= 0 && v <= 2) ctx->panel_mode = v;
+    }
     configure_tc_kernels(ctx);
     configure_solve_kernels(ctx);
     configure_batched_kernels(ctx);

@@ -8,7 +8,7 @@
 // C), here with an FP32 C: every trailing update is applied to the FP32
 // master matrix, only the two input operands are rounded to 16 bits.
 //
-// Kernel: one 128 x 128 output tile per CTA (4 warps).  Warp 0 / lane 0 feeds
+// Kernel: one 128 x 128 output tile per CTA (4 warps), two CTAs per SM.  Warp 0 / lane 0 feeds
 // a STAGES-deep shared-memory ring with TMA tile loads (128 rows x 64
 // elements of A and of B per stage, 128-byte swizzle, no multicast); warp 1 /
 // lane 0 issues tcgen05.mma (kind::f16, M=128, N=128, K=16) into a 128-column
@@ -31,7 +31,7 @@ namespace {
 constexpr int TM = 128;
 constexpr int TN = 128;
 constexpr int TK = 64;  // 64 x 16-bit = 128 bytes = one swizzle row
-constexpr int STAGES = 4;
+constexpr int STAGES = 3;  // 2 CTAs per SM: one's epilogue overlaps the other's main loop
 constexpr int A_BYTES = TM * TK * 2;
 constexpr int B_BYTES = TN * TK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
@@ -120,7 +120,7 @@ struct TcArgs {
     int* err;
 };
 
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
 tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                    const TcArgs args)
 {

@@ -1,0 +1,100 @@
+"""Per-stage profile of one factorization (the role of the reference's
+``profile_double_blocked_potrf`` / ``profile_double_blocked_getrf``
+executables, src/potrf/benchmark/profile_double_blocked_potrf.cpp and
+src/getrf/benchmark/profile_double_blocked_getrf.cpp).
+
+    python -m hygondoubleblockedfactorizations_b200.stage_profile \\
+        --op getrf --precision fp32 --n 8192 --outer 8192 --inner 512 [--reps 1]
+
+Builds the seeded input on the device (POTRF: (A + A^T)/2 + n I from the
+counter-based U[-1,1) stream; GETRF: U[-1,1)), runs one warm-up call (which
+also records the call's profiled CUDA graph), then ``reps`` profiled calls, and prints
+one JSON line: total time, TFLOP/s (n^3/3 or 2n^3/3) and, per kernel class,
+launches, milliseconds, share of the device time and TFLOP/s or GB/s.
+``--panel`` selects the GETRF panel kernel (0 automatic, 1 grid-wide,
+2 cluster).  Mixed precisions use ``hdbf_spotrf_mixed`` / ``hdbf_sgetrf_mixed``
+with panel width ``--inner``.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+
+
+def main(argv=None):
+    import torch
+
+    from . import PREC, Handle, call, lib
+    from .tuner import _matrix
+
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--op", choices=["potrf", "getrf"], default="getrf")
+    ap.add_argument("--precision", choices=list(PREC), default="fp32")
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--outer", type=int, default=8192)
+    ap.add_argument("--inner", type=int, default=512)
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--panel", type=int, default=None)
+    ap.add_argument("--seed", type=int, default=1)
+    a = ap.parse_args(argv)
+
+    P = ctypes.c_void_p
+    h = Handle(torch.cuda.current_stream().cuda_stream)
+    if a.panel is not None:
+        h.set_panel_kernel(a.panel)
+    n = a.n
+    A0 = _matrix(torch, h, a.op, n, a.seed)
+    A = torch.empty_like(A0)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def run():
+        A.copy_(A0)
+        if a.precision == "fp32" and a.op == "potrf":
+            call("double_blocked_potrf_kblocked_syrk", h.ptr, P(A.data_ptr()), n, n, a.outer,
+                 a.inner, 0, P(info.data_ptr()))
+        elif a.precision == "fp32":
+            call("double_blocked_getrf", h.ptr, P(A.data_ptr()), n, n, a.outer, a.inner, 0, 0,
+                 P(ipiv.data_ptr()), P(info.data_ptr()))
+        elif a.op == "potrf":
+            st = lib().hdbf_spotrf_mixed(h.ptr, PREC[a.precision], P(A.data_ptr()), n, n, a.inner,
+                                         P(info.data_ptr()))
+            assert st == 0, st
+        else:
+            st = lib().hdbf_sgetrf_mixed(h.ptr, PREC[a.precision], P(A.data_ptr()), n, n, a.inner,
+                                         P(ipiv.data_ptr()), P(info.data_ptr()))
+            assert st == 0, st
+
+    # warm-up with the profiler on: records the profiled CUDA graph replayed below
+    h.profile_begin()
+    run()
+    torch.cuda.synchronize()
+    h.profile_end()
+    h.check("warm-up")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h.profile_begin()
+    e0.record()
+    for _ in range(a.reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    prof = h.profile_end()
+    ms = e0.elapsed_time(e1) / a.reps
+    flops = n ** 3 / 3.0 if a.op == "potrf" else 2.0 * n ** 3 / 3.0
+    dev_ms = sum(v[1] for v in prof.values()) / a.reps
+    stages = {}
+    for k, (nl, t, fl, by) in sorted(prof.items(), key=lambda kv: -kv[1][1]):
+        stages[k] = {"launches": nl // a.reps, "ms": round(t / a.reps, 3),
+                     "share": round(t / a.reps / dev_ms, 4) if dev_ms else None,
+                     "tflops": round(fl / (t / 1e3) / 1e12, 3) if fl and t else None,
+                     "gbs": round(by / (t / 1e3) / 1e9, 1) if by and t else None}
+    out = {"op": a.op, "precision": a.precision, "n": n, "outer": a.outer, "inner": a.inner,
+           "panel": a.panel, "ms": round(ms, 3), "tflops": round(flops / (ms / 1e3) / 1e12, 3),
+           "info": int(info.item()), "device_errors": h.device_errors(), "stages": stages}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    main()

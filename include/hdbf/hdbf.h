@@ -89,7 +89,8 @@ hdbf_status hdbf_set_graph_mode(hdbf_handle handle, int enabled);
  * column block fits in one cluster's shared memory, otherwise the
  * grid-wide publish-and-poll kernel), 1 = always the grid-wide kernel,
  * 2 = cluster only (blocks that do not fit still take the grid-wide kernel).
- * Both produce identical pivots and factors. */
+ * Both produce identical pivots and factors.  A new handle starts in the mode
+ * named by the environment variable HDBF_PANEL_KERNEL (0, 1 or 2), else 0. */
 hdbf_status hdbf_set_panel_kernel(hdbf_handle handle, int mode);
 
 /* Per-launch event profiling of this library's kernels on the handle's

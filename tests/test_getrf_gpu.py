@@ -224,3 +224,35 @@ def test_graph_replay_getrf(hd, handle, torch_cuda):
         np.testing.assert_array_equal(o[1], outs[0][1])
         assert o[2] == 0
     np.testing.assert_array_equal(outs[0][1], oracle.lapack_sgetrf(G)[1])
+
+
+def test_panel_kernels_agree_bitwise_large(hd, handle, torch_cuda):
+    """n = 16384: the first panels run on 16-CTA clusters, later ones on 8, 4,
+    2 and 1; the grid-wide kernel must give bit-identical factors and pivots
+    (same arithmetic, same order).  Pivots follow host sgetrf up to FP32
+    near-ties; the residual is the FP64 ||PA - LU||_F / ||A||_F (GPU FP64,
+    same formula as the oracle), scaled by n * eps32."""
+    n = 16384
+    G = oracle.general_uniform(n, 1)
+    out = {}
+    for panel in (0, 1):
+        handle.set_panel_kernel(panel)
+        dA, _, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf",
+                                      outer=4096, inner=512)
+        assert info == 0 and handle.device_errors() == 0
+        out[panel] = (dA.clone(), ipiv)
+    assert np.array_equal(out[0][1], out[1][1])
+    assert torch_cuda.equal(out[0][0], out[1][0])
+    ipiv = out[0][1]
+    assert_pivots_match(G, ipiv, oracle.lapack_sgetrf(G)[1], "host sgetrf")
+    torch = torch_cuda
+    LU = out[0][0].view(n, n).t().double()  # row-major view of the column-major factor
+    L = torch.tril(LU, -1) + torch.eye(n, dtype=torch.float64, device="cuda")
+    U = torch.triu(LU)
+    A = torch.from_numpy(np.ascontiguousarray(G)).cuda().double()
+    perm = np.arange(n)
+    for i, p in enumerate(ipiv - 1):
+        perm[i], perm[p] = perm[p], perm[i]
+    PA = A[torch.from_numpy(perm).cuda()]
+    r = (torch.linalg.matrix_norm(PA - L @ U) / torch.linalg.matrix_norm(A)).item()
+    assert r / (n * 2.0 ** -23) <= BOUND, r
