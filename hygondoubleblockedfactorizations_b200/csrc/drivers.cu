@@ -9,7 +9,7 @@ namespace hdbf {
 
 namespace {
 constexpr int kDiagLeaf = 64;   // potf2_small / trsm_*_small leaf order
-constexpr int kPanelLeaf = 32;  // getf2_coop width
+constexpr int kClusterLeaf = 32;  // widest block of the cluster panel kernel
 
 // Split point for a recursion on `n` columns with `leaf`-aligned halves.
 inline int split_at(int n, int leaf)
@@ -108,22 +108,25 @@ hdbf_status getrf_workspace(hdbf_context* ctx, int n, GetrfWs* ws)
     return HDBF_STATUS_SUCCESS;
 }
 
-// Recursive (Toledo/Gustavson) LU of an m x w panel; leaves of kPanelLeaf
-// columns go to the cooperative kernel.  ipiv receives (local row + 1 +
-// ipiv_add) for the panel's w columns.
+// Recursive (Toledo/Gustavson) LU of an m x w panel.  Leaves are column
+// blocks of the handle's panel-leaf width (default 128; 32 when the cluster
+// kernel is forced) and go to the cluster kernel when they fit in one cluster
+// (w <= 32), otherwise to the grid-wide kernel.  ipiv receives (local row + 1
+// + ipiv_add) for the panel's w columns.
 hdbf_status getrf_panel(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
                         int ipiv_add, int* info, int info_base, bool pivot, const GetrfWs& ws)
 {
     if (m <= 0 || w <= 0) return HDBF_STATUS_SUCCESS;
-    if (w <= kPanelLeaf) {
-        if (ctx->panel_mode != 1) {
+    const int leaf = ctx->panel_mode == 2 ? kClusterLeaf : ctx->panel_leaf;
+    if (w <= leaf) {
+        if (ctx->panel_mode != 1 && w <= kClusterLeaf) {
             const hdbf_status st =
                 getf2_cluster(ctx, m, w, A, lda, ipiv, ipiv_add, info, info_base, pivot);
             if (st != HDBF_STATUS_NOT_SUPPORTED) return st;
         }
         return getf2_coop(ctx, m, w, A, lda, ipiv, ipiv_add, info, info_base, pivot);
     }
-    const int w1 = split_at(w, kPanelLeaf);
+    const int w1 = split_at(w, leaf);
     const int w2 = w - w1;
     HDBF_TRY(getrf_panel(ctx, m, w1, A, lda, ipiv, ipiv_add, info, info_base, pivot, ws));
     float* A12 = A + (long long)w1 * lda;

@@ -2,7 +2,7 @@
 //
 // getf2_coop replaces rocsolver_sgetrf's unblocked leaf on the tall panel
 // (src/getrf/getrf_pivot_internal.h:17-39): one cooperative launch factors an
-// m x w (w <= 32) column block with partial pivoting.  Each CTA keeps a
+// m x w (w <= 128) column block with partial pivoting.  Each CTA keeps a
 // contiguous slice of rows of the block resident in shared memory; per column
 // the CTAs publish their local |max| candidate (value, row and the full
 // candidate row) and the owner of the diagonal row publishes that row, then
@@ -26,7 +26,7 @@ namespace hdbf {
 namespace {
 
 constexpr int kCoopThreads = 256;
-constexpr int kCoopMaxW = 32;
+constexpr int kCoopMaxW = 128;
 constexpr int kCoopMaxGrid = 256;
 // Per-(parity, CTA) exchange slot: [seq, |val|, row, pad | cand row (32) | diag row (32)]
 constexpr int kSlotFloats = 4 + 2 * kCoopMaxW;
@@ -431,10 +431,15 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     float* scr = ws_coop(ctx);
 
     // Grid: ~512 rows per CTA (fewer CTAs = fewer slots to poll per column),
-    // at most one CTA per SM; co-residency is guaranteed by the cooperative
-    // launch, which fails instead of hanging if the grid cannot fit.
+    // more when the slice would not fit in shared memory, at most one CTA per
+    // SM; co-residency is guaranteed by the cooperative launch, which fails
+    // instead of hanging if the grid cannot fit.
     const size_t smem_cap = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
-    int G = (m + 511) / 512;
+    const size_t row_bytes = (size_t)w * sizeof(float);
+    const long long fit_rows = (long long)(smem_cap / row_bytes);
+    const int target = ctx->panel_rows > 0 ? ctx->panel_rows : 512;
+    int G = (m + target - 1) / target;
+    if (fit_rows > 0 && (m + fit_rows - 1) / fit_rows > G) G = (int)((m + fit_rows - 1) / fit_rows);
     if (G > ctx->sm_count) G = ctx->sm_count;
     if (G > kCoopMaxGrid) G = kCoopMaxGrid;
     if (G < 1) G = 1;

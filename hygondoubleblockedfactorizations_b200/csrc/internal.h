@@ -53,6 +53,8 @@ struct hdbf_context {
     size_t max_smem_optin = 0;
     int cluster_max = 0;  // largest cluster the panel kernel can launch (0: none)
     int panel_mode = 0;   // hdbf_set_panel_kernel
+    int panel_leaf = 128; // GETRF panel recursion leaf width (32, 64 or 128)
+    int panel_rows = 512; // target rows per CTA of the grid-wide panel kernel
     // Workspace arena (grown on demand outside stream capture).
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -208,7 +210,7 @@ size_t wave_scratch_bytes(int n);
 void configure_wave_kernels(hdbf_context* ctx);
 void configure_batched_kernels(hdbf_context* ctx);
 
-// Cooperative partially pivoted LU of an m x w panel (w <= 32).  Pivots are
+// Cooperative partially pivoted LU of an m x w panel (w <= 128).  Pivots are
 // written 1-based as (local row + 1 + ipiv_add).
 hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
                        int ipiv_add, int* info, int info_base, bool pivot);

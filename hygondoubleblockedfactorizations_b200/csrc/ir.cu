@@ -203,6 +203,25 @@ int next_precision(int prec)
     }
 }
 
+// Block sizes of the refinement's factorization: the fastest candidates of
+// the exhaustive B200 sweep over n = 1024..32768 (the selector's training
+// records).  FP32 POTRF: (2048, 256) below n = 16384, else (4096, 512).
+// FP32 GETRF: (8192, 1024).  Mixed panel width: 256 below n = 12288, then
+// 512, and 1024 from n = 16384 (GETRF) or n = 28672 (POTRF).
+struct IrBlocks {
+    int outer, inner;
+};
+IrBlocks ir_blocks(bool spd, int prec, int n)
+{
+    if (prec == HDBF_PREC_FP32) {
+        if (spd) return n < 16384 ? IrBlocks{2048, 256} : IrBlocks{4096, 512};
+        return IrBlocks{8192, 1024};
+    }
+    const int wide = spd ? 28672 : 16384;
+    const int nb = n < 12288 ? 256 : (n < wide ? 512 : 1024);
+    return IrBlocks{nb, nb};
+}
+
 class IrSolver {
 public:
     IrSolver(hdbf_context* ctx, bool spd, const double* A, long long lda, int n, int nrhs,
@@ -217,16 +236,19 @@ public:
         d2s_kernel<<<g, 256, 0, s>>>(A_, lda_, b_.W, n_, n_, n_);
         ctx_->launches++;
         HDBF_TRY(last_cuda(ctx_));
-        const int nb = 512;
+        const IrBlocks blk = ir_blocks(spd_, prec, n_);
         if (prec == HDBF_PREC_FP32) {
-            if (spd_) double_blocked_potrf_kblocked_syrk(ctx_, b_.W, n_, n_, 4096, nb, 0, b_.info);
-            else double_blocked_getrf(ctx_, b_.W, n_, n_, 8192, nb, getrf_outer_trsm_direct, 0,
-                                      b_.ipiv, b_.info);
+            if (spd_)
+                double_blocked_potrf_kblocked_syrk(ctx_, b_.W, n_, n_, blk.outer, blk.inner, 0,
+                                                   b_.info);
+            else
+                double_blocked_getrf(ctx_, b_.W, n_, n_, blk.outer, blk.inner,
+                                     getrf_outer_trsm_direct, 0, b_.ipiv, b_.info);
             HDBF_TRY(ctx_->last_status);
         } else if (spd_) {
-            HDBF_TRY(potrf_mixed(ctx_, prec, b_.W, n_, n_, nb, b_.info));
+            HDBF_TRY(potrf_mixed(ctx_, prec, b_.W, n_, n_, blk.inner, b_.info));
         } else {
-            HDBF_TRY(getrf_mixed(ctx_, prec, b_.W, n_, n_, nb, b_.ipiv, b_.info));
+            HDBF_TRY(getrf_mixed(ctx_, prec, b_.W, n_, n_, blk.inner, b_.ipiv, b_.info));
         }
         if (!spd_) HDBF_TRY(ipiv_to_perm(ctx_, b_.ipiv, n_, b_.perm));
         if (cudaMemcpyAsync(host_info, b_.info, sizeof(int), cudaMemcpyDeviceToHost, s) !=
@@ -343,7 +365,7 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
     if (max_iter < 0) max_iter = 0;
     HDBF_TRY(ensure_ws(ctx, n));
     // One arena for the shadows (offset 0) and the refinement buffers.
-    const size_t shadow = mixed_shadow_bytes(n, 512, true);
+    const size_t shadow = mixed_shadow_bytes(n, 1024, true);  // widest panel ir_blocks picks
     hdbf_status st;
     char* arena = static_cast<char*>(mixed_arena(ctx, shadow + ir_bytes(n, nrhs), &st));
     if (!arena) return st;

@@ -26,6 +26,8 @@
 
 namespace hdbf {
 
+size_t mixed_base_bytes(int n, int b);
+
 namespace {
 
 inline long long pad8(long long x) { return (x + 7) / 8 * 8; }
@@ -90,6 +92,61 @@ __global__ void absmax_kernel(const float* A, long long lda, int rows, int cols,
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(v));
 }
 
+__global__ void set_identity_kernel(float* W, long long ldw, int n)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const long long c = blockIdx.y;
+    if (r < n) W[c * ldw + r] = (r == c) ? 1.f : 0.f;
+}
+
+hdbf_status set_identity(hdbf_context* ctx, float* W, long long ldw, int n)
+{
+    dim3 g((n + 255) / 256, n);
+    set_identity_kernel<<<g, 256, 0, ctx->stream>>>(W, ldw, n);
+    ctx->launches++;
+    return last_cuda(ctx);
+}
+
+hdbf_status zero_block(hdbf_context* ctx, float* A, long long lda, int rows, int cols)
+{
+    if (rows <= 0 || cols <= 0) return HDBF_STATUS_SUCCESS;
+    if (cudaMemset2DAsync(A, (size_t)lda * sizeof(float), 0, (size_t)rows * sizeof(float), cols,
+                          ctx->stream) != cudaSuccess)
+        return last_cuda(ctx);
+    return HDBF_STATUS_SUCCESS;
+}
+
+// Panel TRSM of the mixed factorizations.  BF16 and FP16 modes: one
+// tensor-core GEMM with the FP32 inverse block, BF16 operands (FP32 range, so
+// the inverse needs no scaling); one product in BF16 mode, hi + lo split
+// (three products, ~16 significant bits) in FP16 mode.  The split modes keep
+// the FP32 TRSM: their factors must be accurate to ~2^-22, which 16-bit
+// operands of an unscaled inverse cannot give.
+bool trsm_on_tc(const PrecInfo& pi) { return !pi.split; }
+PrecInfo trsm_prec(const PrecInfo& pi) { return {kFmtBF16, pi.fmt == kFmtF16}; }
+
+// Inverse-block scratch inside the arena.
+struct WBlock {
+    float* W;
+    long long ldw;
+    void* wh;
+    void* wl;
+    long long ldws;
+};
+WBlock w_block(char* arena, int n, int b)
+{
+    WBlock w;
+    char* p = arena + mixed_base_bytes(n, b);
+    w.W = reinterpret_cast<float*>(p);
+    w.ldw = pad8(b);
+    p += align_up((size_t)b * pad8(b) * 4, 256);
+    w.wh = p;
+    p += align_up((size_t)b * pad8(b) * 2, 256);
+    w.wl = p;
+    w.ldws = pad8(b);
+    return w;
+}
+
 }  // namespace
 
 // max |A| (diag_only: max |A(i,i)|); synchronises the stream.
@@ -121,9 +178,15 @@ float shadow_scale(int fmt, float maxabs)
     return std::ldexp(1.f, std::max(-60, std::min(60, e)));
 }
 
+// Arena: four n x pad8(b) 16-bit shadows (hi/lo of two operands; the
+// panel-TRSM GEMM uses the lo halves as scratch in every mode), then the
+// FP32 inverse block W (b x pad8(b)) and its hi/lo shadows.
+size_t mixed_base_bytes(int n, int b) { return align_up((size_t)4 * n * pad8(b) * 2, 256); }
 size_t mixed_shadow_bytes(int n, int b, bool split)
 {
-    return (size_t)(split ? 4 : 2) * (size_t)n * pad8(b) * 2 + 1024;
+    (void)split;
+    const size_t w = align_up((size_t)b * pad8(b) * 4, 256) + 2 * align_up((size_t)b * pad8(b) * 2, 256);
+    return mixed_base_bytes(n, b) + w + 1024;
 }
 
 // Right-looking mixed Cholesky (lower) with block b; shadows in `arena`.
@@ -136,7 +199,10 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
     const size_t one = (size_t)n * lds * 2;
     void* hi = arena;
     void* lo = pi.split ? arena + one : nullptr;
+    void* scratch_lo = arena + one;
     const float inv_s2 = 1.f / (s * s);
+    const PrecInfo tp = trsm_prec(pi);
+    const WBlock wb = w_block(arena, n, b);
     if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int k = 0; k < n; k += b) {
         const int psz = std::min(b, n - k);
@@ -145,7 +211,25 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         HDBF_TRY(potrf_diag(ctx, psz, Akk, lda, info, k));
         if (tr <= 0) continue;
         float* A21 = at(A, lda, k + psz, k);
-        HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
+        // L21 = A21 L11^{-T} as one tensor-core GEMM: W = L11^{-T} is the
+        // FP32 TRSM of the identity; A21 is rounded into the shadow and
+        // overwritten with the product.
+        if (!trsm_on_tc(pi)) {
+            HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
+            HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, s));
+            HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
+                               at(A, lda, k + psz, k + psz), lda, inv_s2, true));
+            continue;
+        }
+        HDBF_TRY(set_identity(ctx, wb.W, wb.ldw, psz));
+        HDBF_TRY(trsm_rlt(ctx, psz, psz, Akk, lda, wb.W, wb.ldw));
+        HDBF_TRY(convert_direct16(ctx, tp.fmt, psz, psz, wb.W, wb.ldw, wb.wh,
+                                  tp.split ? wb.wl : nullptr, wb.ldws, 1.f));
+        HDBF_TRY(convert_transpose16(ctx, tp.fmt, tr, psz, A21, lda, hi,
+                                     tp.split ? scratch_lo : nullptr, lds, 1.f));
+        HDBF_TRY(zero_block(ctx, A21, lda, tr, psz));
+        HDBF_TRY(tc_update(ctx, tp, tr, psz, psz, hi, scratch_lo, lds, wb.wh, wb.wl, wb.ldws, A21,
+                           lda, -1.f, false));
         HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, s));
         HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
                            at(A, lda, k + psz, k + psz), lda, inv_s2, true));
@@ -167,6 +251,9 @@ hdbf_status getrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
     void* hU = arena + one;
     void* lL = pi.split ? arena + 2 * one : nullptr;
     void* lU = pi.split ? arena + 3 * one : nullptr;
+    void* scratch_lo = arena + 3 * one;
+    const PrecInfo tp = trsm_prec(pi);
+    const WBlock wb = w_block(arena, n, b);
     const float inv_s = 1.f / (sL * sU);
     if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int p = 0; p < n; p += b) {
@@ -185,7 +272,22 @@ hdbf_status getrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         if (tr <= 0) continue;
         HDBF_TRY(apply_moves(ctx, at(A, lda, p, next), lda, tr, ws.src, ws.tgt, ws.count,
                              max_moves, ws.temp, ws.temp_cols));
-        HDBF_TRY(trsm_llu(ctx, psz, tr, at(A, lda, p, p), lda, at(A, lda, p, next), lda));
+        // U12 = L11^{-1} A12 as one tensor-core GEMM: W = L11^{-1} (unit lower)
+        // is the FP32 TRSM of the identity.
+        float* A12 = at(A, lda, p, next);
+        if (trsm_on_tc(pi)) {
+            HDBF_TRY(set_identity(ctx, wb.W, wb.ldw, psz));
+            HDBF_TRY(trsm_llu(ctx, psz, psz, at(A, lda, p, p), lda, wb.W, wb.ldw));
+            HDBF_TRY(convert_transpose16(ctx, tp.fmt, psz, psz, wb.W, wb.ldw, wb.wh,
+                                         tp.split ? wb.wl : nullptr, wb.ldws, 1.f));
+            HDBF_TRY(convert_direct16(ctx, tp.fmt, psz, tr, A12, lda, hU,
+                                      tp.split ? scratch_lo : nullptr, lds, 1.f));
+            HDBF_TRY(zero_block(ctx, A12, lda, psz, tr));
+            HDBF_TRY(tc_update(ctx, tp, psz, tr, psz, wb.wh, wb.wl, wb.ldws, hU, scratch_lo, lds,
+                               A12, lda, -1.f, false));
+        } else {
+            HDBF_TRY(trsm_llu(ctx, psz, tr, at(A, lda, p, p), lda, A12, lda));
+        }
         HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, at(A, lda, next, p), lda, hL, lL, lds,
                                      sL));
         HDBF_TRY(convert_direct16(ctx, pi.fmt, psz, tr, at(A, lda, p, next), lda, hU, lU, lds, sU));

@@ -335,6 +335,14 @@ hdbf_status hdbf_create(hdbf_handle* handle)
         const int v = std::atoi(pk);
         if (v >= 0 && v <= 2) ctx->panel_mode = v;
     }
+    if (const char* pl = std::getenv("HDBF_PANEL_LEAF")) {  // default panel leaf width
+        const int v = std::atoi(pl);
+        if (v == 32 || v == 64 || v == 128) ctx->panel_leaf = v;
+    }
+    if (const char* pr = std::getenv("HDBF_PANEL_ROWS")) {  // rows per panel CTA
+        const int v = std::atoi(pr);
+        if (v >= 64 && v <= 4096) ctx->panel_rows = v;
+    }
     configure_tc_kernels(ctx);
     configure_solve_kernels(ctx);
     configure_batched_kernels(ctx);

@@ -90,7 +90,12 @@ hdbf_status hdbf_set_graph_mode(hdbf_handle handle, int enabled);
  * grid-wide publish-and-poll kernel), 1 = always the grid-wide kernel,
  * 2 = cluster only (blocks that do not fit still take the grid-wide kernel).
  * Both produce identical pivots and factors.  A new handle starts in the mode
- * named by the environment variable HDBF_PANEL_KERNEL (0, 1 or 2), else 0. */
+ * named by the environment variable HDBF_PANEL_KERNEL (0, 1 or 2), else 0.
+ * The panel recursion stops at leaves of 128 columns (the grid-wide kernel
+ * takes up to 128; the cluster kernel up to 32, so mode 2 recurses to 32);
+ * HDBF_PANEL_LEAF (32, 64 or 128) sets a new handle's leaf width, and
+ * HDBF_PANEL_ROWS (64..4096, default 512) the rows each CTA of the grid-wide
+ * kernel aims to hold. */
 hdbf_status hdbf_set_panel_kernel(hdbf_handle handle, int mode);
 
 /* Per-launch event profiling of this library's kernels on the handle's
