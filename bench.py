@@ -263,38 +263,50 @@ def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
         mats[key] = (A, B)
         return A, B
 
+    def run(kind, A, B, X, prec, method):
+        if method == "gmres":
+            fn = "hdbf_dposv_mixed_gmres" if kind == "spd" else "hdbf_dgesv_mixed_gmres"
+        else:
+            fn = "hdbf_dposv_mixed" if kind == "spd" else "hdbf_dgesv_mixed"
+        info = hd.IrInfo()
+        if method == "gmres":
+            args = (handle.ptr, hd.PREC[prec], A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
+                    X.data_ptr(), n, ctypes.c_double(1e-13), 10, 30, ctypes.c_double(1e-4),
+                    ctypes.byref(info))
+        else:
+            args = (handle.ptr, hd.PREC[prec], 1, A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
+                    X.data_ptr(), n, ctypes.c_double(1e-13), 30, ctypes.byref(info))
+        hd.call(fn, *args)  # builds the graphs and the workspace
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = hd.call(fn, *args)
+        e1.record()
+        torch.cuda.synchronize()
+        return {"method": method, "precision": prec, "ms": round(e0.elapsed_time(e1), 2),
+                "status": int(st), "converged": int(info.converged),
+                "iterations": int(info.iterations), "inner_iterations": int(info.inner_iterations),
+                "backward_error": float(info.backward_error),
+                "final_precision": int(info.final_precision),
+                "factorizations": int(info.factorizations),
+                "factor_ms": round(info.factor_ms, 2), "refine_ms": round(info.refine_ms, 2)}
+
     fp32_done = {}
-    for kind, kappa, prec in cases:
+    for kind, kappa, prec, method in cases:
         A, B = matrix(kind, kappa)
         X = torch.zeros(nrhs, n, dtype=torch.float64, device="cuda")
-        fn = "hdbf_dposv_mixed" if kind == "spd" else "hdbf_dgesv_mixed"
-        res = {}
-        if (kind, kappa) in fp32_done:
-            res["fp32"] = fp32_done[(kind, kappa)]
-        for p in ("fp32", prec):
-            if p in res:
-                continue
-            info = hd.IrInfo()
-            args = (handle.ptr, hd.PREC[p], 1, A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
-                    X.data_ptr(), n, ctypes.c_double(1e-13), 30, ctypes.byref(info))
-            hd.call(fn, *args)  # builds the graphs and the workspace
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            st = hd.call(fn, *args)
-            e1.record()
-            torch.cuda.synchronize()
-            res[p] = {"ms": round(e0.elapsed_time(e1), 2), "status": int(st),
-                      "converged": int(info.converged), "iterations": int(info.iterations),
-                      "backward_error": float(info.backward_error),
-                      "final_precision": int(info.final_precision),
-                      "factorizations": int(info.factorizations),
-                      "factor_ms": round(info.factor_ms, 2), "refine_ms": round(info.refine_ms, 2)}
-        fp32_done[(kind, kappa)] = res["fp32"]
+        if (kind, kappa) not in fp32_done:
+            # FP32 reference: the faster converged of classical IR and GMRES-IR
+            cand = [run(kind, A, B, X, "fp32", mth) for mth in ("ir", "gmres")]
+            ok = [c for c in cand if c["converged"] and c["backward_error"] <= 1e-13]
+            fp32_done[(kind, kappa)] = (min(ok, key=lambda c: c["ms"]) if ok else
+                                        min(cand, key=lambda c: c["ms"]), cand)
+        r32, alts = fp32_done[(kind, kappa)]
+        rm = run(kind, A, B, X, prec, method)
         flops = (n ** 3 / 3.0) if kind == "spd" else (2.0 * n ** 3 / 3.0)
-        r32, rm = res["fp32"], res[prec]
-        out[f"{'potrf' if kind == 'spd' else 'getrf'}_k{kappa:.0e}_{prec}"] = {
-            "fp32_ir": r32, "mixed_ir": rm,
+        key = f"{'potrf' if kind == 'spd' else 'getrf'}_k{kappa:.0e}_{prec}_{method}"
+        out[key] = {
+            "fp32_ir": r32, "fp32_alternatives": alts, "mixed_ir": rm,
             "speedup_time_to_solution": round(r32["ms"] / rm["ms"], 3) if rm["ms"] > 0 else None,
             "mixed_effective_tflops": round(flops / (rm["ms"] / 1e3) / 1e12, 2),
             "fp32_effective_tflops": round(flops / (r32["ms"] / 1e3) / 1e12, 2)}
@@ -429,8 +441,10 @@ def run_ours(args, rank, world):
 
     mixed = None
     if not args.skip_mixed and world == 1:
-        cases = [("spd", 1e2, "bf16"), ("spd", 1e2, "fp16"), ("gen", 1e2, "bf16"),
-                 ("gen", 1e2, "fp16"), ("spd", 1e6, "fp16x3"), ("gen", 1e6, "fp16x3")]
+        cases = [("spd", 1e2, "bf16", "ir"), ("spd", 1e2, "fp16", "ir"),
+                 ("gen", 1e2, "fp16", "gmres"), ("gen", 1e2, "bf16", "gmres"),
+                 ("gen", 1e4, "fp16", "gmres"),
+                 ("spd", 1e6, "fp16x3", "ir"), ("gen", 1e6, "fp16x3", "gmres")]
         mixed = mixed_ir_cases(torch, hd, handle, n, cases)
         best = {}
         for key, v in mixed.items():

@@ -88,6 +88,10 @@ _PROTOS = {
                                  c_double, c_int, P]),
     "hdbf_dgesv_mixed": (c_int, [P, c_int, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
                                  c_double, c_int, P]),
+    "hdbf_dposv_mixed_gmres": (c_int, [P, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
+                                       c_double, c_int, c_int, c_double, P]),
+    "hdbf_dgesv_mixed_gmres": (c_int, [P, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
+                                       c_double, c_int, c_int, c_double, P]),
     "hdbf_selector_num_params": (c_int, [c_int, c_int]),
     "hdbf_selector_init": (c_int, [P, P, c_int, c_int, c_ull]),
     "hdbf_selector_train": (c_int, [P, P, P, P, c_int, P, P, P, c_int, c_int, c_int, c_int,
@@ -113,7 +117,8 @@ class IrInfo(ctypes.Structure):
     """hdbf_ir_info (include/hdbf/mixed.h)."""
     _fields_ = [("iterations", c_int), ("converged", c_int), ("final_precision", c_int),
                 ("factorizations", c_int), ("info", c_int), ("backward_error", c_double),
-                ("history", c_double * 64), ("factor_ms", c_double), ("refine_ms", c_double)]
+                ("history", c_double * 64), ("factor_ms", c_double), ("refine_ms", c_double),
+                ("inner_iterations", c_int)]
 
 
 class HdbfError(RuntimeError):

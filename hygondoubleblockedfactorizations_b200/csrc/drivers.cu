@@ -25,6 +25,7 @@ hdbf_status potrf_diag(hdbf_context* ctx, int n, float* A, long long lda, int* i
 {
     if (n <= 0) return HDBF_STATUS_SUCCESS;
     if (n <= kDiagLeaf) return potf2_small(ctx, n, A, lda, info, info_base);
+    if (n <= potrf_block_max_n()) return potrf_block(ctx, n, A, lda, info, info_base, nullptr, 0);
     const int n1 = split_at(n, kDiagLeaf);
     const int n2 = n - n1;
     float* A21 = A + n1;

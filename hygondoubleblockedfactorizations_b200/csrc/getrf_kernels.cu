@@ -430,14 +430,14 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     HDBF_TRY(ensure_ws(ctx, 64));
     float* scr = ws_coop(ctx);
 
-    // Grid: ~512 rows per CTA (fewer CTAs = fewer slots to poll per column),
+    // Grid: ~256 rows per CTA (panel_rows; measured fastest at n = 32768),
     // more when the slice would not fit in shared memory, at most one CTA per
     // SM; co-residency is guaranteed by the cooperative launch, which fails
     // instead of hanging if the grid cannot fit.
     const size_t smem_cap = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
     const size_t row_bytes = (size_t)w * sizeof(float);
     const long long fit_rows = (long long)(smem_cap / row_bytes);
-    const int target = ctx->panel_rows > 0 ? ctx->panel_rows : 512;
+    const int target = ctx->panel_rows > 0 ? ctx->panel_rows : 256;
     int G = (m + target - 1) / target;
     if (fit_rows > 0 && (m + fit_rows - 1) / fit_rows > G) G = (int)((m + fit_rows - 1) / fit_rows);
     if (G > ctx->sm_count) G = ctx->sm_count;

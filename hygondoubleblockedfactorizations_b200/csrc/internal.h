@@ -27,7 +27,8 @@ enum KernelClass {
     kClsSkinny = 13,   // skinny_kernel (updates with N <= 32)
     kClsBatched = 14,  // batched_factor_solve_kernel
     kClsSelector = 15, // selector MLP kernels
-    kNumClasses = 16
+    kClsPotrfBlock = 16, // potrf_block_kernel (cooperative diagonal-block Cholesky)
+    kNumClasses = 17
 };
 struct ProfRec {
     int cls;
@@ -54,7 +55,7 @@ struct hdbf_context {
     int cluster_max = 0;  // largest cluster the panel kernel can launch (0: none)
     int panel_mode = 0;   // hdbf_set_panel_kernel
     int panel_leaf = 128; // GETRF panel recursion leaf width (32, 64 or 128)
-    int panel_rows = 512; // target rows per CTA of the grid-wide panel kernel
+    int panel_rows = 256; // target rows per CTA of the grid-wide panel kernel
     // Workspace arena (grown on demand outside stream capture).
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -92,6 +93,7 @@ constexpr int kSmallMoveCount = 12;  // move count of the last composed permutat
 constexpr int kSmallEpoch = 16;      // panel-kernel exchange epoch
 constexpr int kSmallDone = 20;       // panel-kernel finished-CTA counter
 constexpr int kSmallScratch = 24;    // host-read reduction results (absmax etc.)
+constexpr int kSmallBlockBar = 32;   // diagonal-block kernel: barrier counter, fail, abort
 constexpr int kSmallInts = 64;
 
 // Device error codes written into dev_small[kSmallErr].
@@ -262,6 +264,11 @@ hdbf_status fill_uniform(hdbf_context* ctx, float* x, size_t count, uint64_t see
 hdbf_status add_damping(cudaStream_t s, float* A, int n, long long lda, float lambda);
 
 // ---------------------------------------------------------------- drivers
+// Cholesky of an n x n (n <= potrf_block_max_n()) diagonal block in one
+// cooperative launch; with W non-null also W = L^{-1} (lower, upper zeroed).
+hdbf_status potrf_block(hdbf_context* ctx, int n, float* A, long long lda, int* info,
+                        int info_base, float* W, long long ldw);
+int potrf_block_max_n();
 hdbf_status potrf_diag(hdbf_context* ctx, int n, float* A, long long lda, int* info,
                        int info_base);
 hdbf_status trsm_rlt(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,

@@ -149,6 +149,93 @@ __global__ void update_x_kernel(const float* __restrict__ F, long long ldf,
     *x = accumulate ? *x + d : d;
 }
 
+// ---- GMRES-IR kernels (FP64; vector block j of V at V + j * vstride, column c
+// at + c * n)
+constexpr int kDotChunks = 64;
+
+// Y(r, c) = sum_s partial[s][c][r]  (the product A X of resid_partial_kernel)
+__global__ void matvec_final_kernel(const double* __restrict__ partial, double* Y, int n, int nrhs)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    double acc = 0.0;
+    for (int s = 0; s < kSplits; ++s) acc += partial[((long long)s * nrhs + c) * n + r];
+    Y[(long long)c * n + r] = acc;
+}
+
+// partial[(j * nrhs + c) * kDotChunks + chunk] = sum over the chunk's rows of
+// V_j(r, c) * Wv(r, c); fixed-order tree reduction (deterministic).
+__global__ void __launch_bounds__(256) dot_partial_kernel(const double* __restrict__ V,
+                                                          long long vstride,
+                                                          const double* __restrict__ Wv, int n,
+                                                          int nrhs, double* partial)
+{
+    __shared__ double red[256];
+    const int chunk = blockIdx.x, j = blockIdx.y, c = blockIdx.z;
+    const int per = (n + kDotChunks - 1) / kDotChunks;
+    const int r0 = chunk * per, r1 = min(n, r0 + per);
+    const double* v = V + (long long)j * vstride + (long long)c * n;
+    const double* w = Wv + (long long)c * n;
+    double acc = 0.0;
+    for (int r = r0 + threadIdx.x; r < r1; r += 256) acc = fma(v[r], w[r], acc);
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if (threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[((long long)j * nrhs + c) * kDotChunks + chunk] = red[0];
+}
+
+// H[j * nrhs + c] = sum over chunks (in order)
+__global__ void dot_final_kernel(const double* __restrict__ partial, int nj, int nrhs, double* H)
+{
+    const int t = blockIdx.x * 256 + threadIdx.x;
+    if (t >= nj * nrhs) return;
+    double acc = 0.0;
+    for (int q = 0; q < kDotChunks; ++q) acc += partial[(long long)t * kDotChunks + q];
+    H[t] = acc;
+}
+
+// Wv(r, c) -= sum_{j < nj} V_j(r, c) H[j * nrhs + c]
+__global__ void axpy_kernel(const double* __restrict__ V, long long vstride, int nj,
+                            const double* __restrict__ H, double* Wv, int n, int nrhs)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    double acc = Wv[(long long)c * n + r];
+    for (int j = 0; j < nj; ++j)
+        acc = fma(-V[(long long)j * vstride + (long long)c * n + r], H[j * nrhs + c], acc);
+    Wv[(long long)c * n + r] = acc;
+}
+
+// Vout(r, c) = Wv(r, c) / sqrt(sq[c])  (0 when sq[c] == 0)
+__global__ void normalize_kernel(const double* __restrict__ Wv, const double* __restrict__ sq,
+                                 double* Vout, int n, int nrhs)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    const double nr = sqrt(sq[c]);
+    Vout[(long long)c * n + r] = nr > 0.0 ? Wv[(long long)c * n + r] / nr : 0.0;
+}
+
+// X(r, c) += sum_{j < nj} V_j(r, c) Y[j * nrhs + c]
+__global__ void combine_kernel(const double* __restrict__ V, long long vstride, int nj,
+                               const double* __restrict__ Y, double* X, long long ldx, int n,
+                               int nrhs)
+{
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n || c >= nrhs) return;
+    double acc = 0.0;
+    for (int j = 0; j < nj; ++j)
+        acc = fma(V[(long long)j * vstride + (long long)c * n + r], Y[j * nrhs + c], acc);
+    X[(long long)c * ldx + r] += acc;
+}
+
 struct IrBuffers {
     float* W = nullptr;      // FP32 working copy / factors (n x n, ld n)
     int* ipiv = nullptr;
@@ -159,18 +246,31 @@ struct IrBuffers {
     float* F2 = nullptr;     // permuted copy for GETRS
     double* part = nullptr;  // kSplits x nrhs x n partial sums
     unsigned long long* nrm = nullptr;  // [0, nrhs): column norms; [nrhs]: ||A||_inf
+    // GMRES-IR (present when m > 0): Krylov basis, A v, dot partials, the
+    // Hessenberg column (h, h2, ||w||^2) and the least-squares solution.
+    int m = 0;
+    double* V = nullptr;     // (m + 1) blocks of n x nrhs
+    double* T = nullptr;     // n x nrhs
+    double* dpart = nullptr; // kDotChunks x (m + 1) x nrhs
+    double* Hd = nullptr;    // 2 (m + 1) nrhs + nrhs doubles
+    double* Yd = nullptr;    // (m + 1) x nrhs
 };
 
 inline size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
-size_t ir_bytes(int n, int nrhs)
+size_t ir_bytes(int n, int nrhs, int m = 0)
 {
-    return al((size_t)n * n * 4) + 3 * al((size_t)n * 4) + al(64) + al((size_t)n * nrhs * 8) +
-           2 * al((size_t)n * nrhs * 4) + al((size_t)kSplits * nrhs * n * 8) +
-           al((size_t)(nrhs + 1) * 8) + 4096;
+    size_t b = al((size_t)n * n * 4) + 3 * al((size_t)n * 4) + al(64) + al((size_t)n * nrhs * 8) +
+               2 * al((size_t)n * nrhs * 4) + al((size_t)kSplits * nrhs * n * 8) +
+               al((size_t)(nrhs + 1) * 8) + 4096;
+    if (m > 0)
+        b += al((size_t)(m + 1) * n * nrhs * 8) + al((size_t)n * nrhs * 8) +
+             al((size_t)kDotChunks * (m + 1) * nrhs * 8) + al((size_t)(2 * (m + 1) + 1) * nrhs * 8) +
+             al((size_t)(m + 1) * nrhs * 8);
+    return b;
 }
 
-IrBuffers carve(char* base, int n, int nrhs)
+IrBuffers carve(char* base, int n, int nrhs, int m = 0)
 {
     IrBuffers b;
     size_t off = 0;
@@ -189,6 +289,14 @@ IrBuffers carve(char* base, int n, int nrhs)
     b.F2 = reinterpret_cast<float*>(take((size_t)n * nrhs * 4));
     b.part = reinterpret_cast<double*>(take((size_t)kSplits * nrhs * n * 8));
     b.nrm = reinterpret_cast<unsigned long long*>(take((size_t)(nrhs + 1) * 8));
+    if (m > 0) {
+        b.m = m;
+        b.V = reinterpret_cast<double*>(take((size_t)(m + 1) * n * nrhs * 8));
+        b.T = reinterpret_cast<double*>(take((size_t)n * nrhs * 8));
+        b.dpart = reinterpret_cast<double*>(take((size_t)kDotChunks * (m + 1) * nrhs * 8));
+        b.Hd = reinterpret_cast<double*>(take((size_t)(2 * (m + 1) + 1) * nrhs * 8));
+        b.Yd = reinterpret_cast<double*>(take((size_t)(m + 1) * nrhs * 8));
+    }
     return b;
 }
 
@@ -263,6 +371,13 @@ public:
     // d = A^{-1} v with the FP32 factors; v scaled column-wise by nrm.
     hdbf_status correction(const double* V, long long ldv, bool accumulate)
     {
+        return precond(V, ldv, X_, ldx_, accumulate);
+    }
+
+    // Out (+)= M^{-1} V, M the low-precision factorization (FP32 solves of the
+    // column-scaled V).
+    hdbf_status precond(const double* V, long long ldv, double* Out, long long ldo, bool accumulate)
+    {
         cudaStream_t s = ctx_->stream;
         HDBF_TRY(colmax(V, ldv, b_.nrm));
         dim3 g((n_ + 255) / 256, nrhs_);
@@ -276,7 +391,57 @@ public:
             HDBF_TRY(getrs_f32_permuted(ctx_, b_.W, n_, n_, nrhs_, b_.F2, n_));
             sol = b_.F2;
         }
-        update_x_kernel<<<g, 256, 0, s>>>(sol, n_, b_.nrm, X_, ldx_, n_, nrhs_, accumulate ? 1 : 0);
+        update_x_kernel<<<g, 256, 0, s>>>(sol, n_, b_.nrm, Out, ldo, n_, nrhs_, accumulate ? 1 : 0);
+        ctx_->launches++;
+        return last_cuda(ctx_);
+    }
+
+    // Y = A X (FP64, X and Y n x nrhs with leading dimension n)
+    hdbf_status matvec(const double* Xv, double* Y)
+    {
+        cudaStream_t s = ctx_->stream;
+        dim3 g1((n_ + kRowsPerCta - 1) / kRowsPerCta, kSplits, (nrhs_ + kRhsGroup - 1) / kRhsGroup);
+        ProfScope prof(ctx_, kClsIr, 2.0 * (double)n_ * n_ * nrhs_, 8.0 * (double)n_ * n_);
+        resid_partial_kernel<<<g1, kRowsPerCta, 0, s>>>(A_, lda_, Xv, n_, n_, nrhs_, b_.part);
+        dim3 g2((n_ + 255) / 256, nrhs_);
+        matvec_final_kernel<<<g2, 256, 0, s>>>(b_.part, Y, n_, nrhs_);
+        ctx_->launches += 2;
+        return last_cuda(ctx_);
+    }
+
+    // H[j * nrhs + c] = <V_j(:, c), Wv(:, c)> for j < nj
+    hdbf_status dots(const double* V, int nj, const double* Wv, double* H)
+    {
+        cudaStream_t s = ctx_->stream;
+        const long long vs = (long long)n_ * nrhs_;
+        dim3 g(kDotChunks, nj, nrhs_);
+        dot_partial_kernel<<<g, 256, 0, s>>>(V, vs, Wv, n_, nrhs_, b_.dpart);
+        dot_final_kernel<<<(nj * nrhs_ + 255) / 256, 256, 0, s>>>(b_.dpart, nj, nrhs_, H);
+        ctx_->launches += 2;
+        return last_cuda(ctx_);
+    }
+
+    hdbf_status axpy(const double* V, int nj, const double* H, double* Wv)
+    {
+        dim3 g((n_ + 255) / 256, nrhs_);
+        axpy_kernel<<<g, 256, 0, ctx_->stream>>>(V, (long long)n_ * nrhs_, nj, H, Wv, n_, nrhs_);
+        ctx_->launches++;
+        return last_cuda(ctx_);
+    }
+
+    hdbf_status normalize(const double* Wv, const double* sq, double* Vout)
+    {
+        dim3 g((n_ + 255) / 256, nrhs_);
+        normalize_kernel<<<g, 256, 0, ctx_->stream>>>(Wv, sq, Vout, n_, nrhs_);
+        ctx_->launches++;
+        return last_cuda(ctx_);
+    }
+
+    hdbf_status combine(const double* V, int nj, const double* Y)
+    {
+        dim3 g((n_ + 255) / 256, nrhs_);
+        combine_kernel<<<g, 256, 0, ctx_->stream>>>(V, (long long)n_ * nrhs_, nj, Y, X_, ldx_, n_,
+                                                    nrhs_);
         ctx_->launches++;
         return last_cuda(ctx_);
     }
@@ -449,6 +614,177 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
     return st;
 }
 
+// GMRES-IR: x0 = M^{-1} b; per outer step r = b - A x (FP64), then restarted
+// left-preconditioned GMRES on M^{-1} A d = M^{-1} r (FP64 vectors, CGS2,
+// Givens least squares on the host per right-hand side), x += d.
+hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, int lda, int n,
+                        int nrhs, const double* B, int ldb, double* X, int ldx, double tol,
+                        int max_iter, int max_inner, double inner_tol, hdbf_ir_info* out)
+{
+    hdbf_ir_info info;
+    memset(&info, 0, sizeof(info));
+    if (n < 0 || nrhs < 0 || nrhs > 64) return HDBF_STATUS_INVALID_VALUE;
+    if (n == 0 || nrhs == 0) {
+        info.converged = 1;
+        if (out) *out = info;
+        return HDBF_STATUS_SUCCESS;
+    }
+    if (!A || !B || !X || lda < n || ldb < n || ldx < n) return HDBF_STATUS_INVALID_VALUE;
+    if (prec < HDBF_PREC_FP32 || prec > HDBF_PREC_FP16X3) return HDBF_STATUS_INVALID_VALUE;
+    if (max_iter < 0) max_iter = 0;
+    const int m = max_inner <= 0 ? 30 : std::min(max_inner, 60);
+    if (!(inner_tol > 0.0)) inner_tol = 1e-4;
+    HDBF_TRY(ensure_ws(ctx, n));
+    const size_t shadow = mixed_shadow_bytes(n, 1024, true);
+    hdbf_status st;
+    char* arena = static_cast<char*>(mixed_arena(ctx, shadow + ir_bytes(n, nrhs, m), &st));
+    if (!arena) return st;
+    const IrBuffers buf = carve(arena + al(shadow), n, nrhs, m);
+    IrSolver solver(ctx, spd, A, lda, n, nrhs, B, ldb, X, ldx, buf);
+    cudaStream_t strm = ctx->stream;
+
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto timed = [&](double* acc, auto&& fn) -> hdbf_status {
+        cudaEventRecord(e0, strm);
+        const hdbf_status s2 = fn();
+        cudaEventRecord(e1, strm);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        *acc += ms;
+        return s2;
+    };
+    auto to_host = [&](void* dst, const void* src, size_t bytes) -> hdbf_status {
+        if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, strm) != cudaSuccess ||
+            cudaStreamSynchronize(strm) != cudaSuccess) {
+            cudaGetLastError();
+            return HDBF_STATUS_CUDA_ERROR;
+        }
+        return HDBF_STATUS_SUCCESS;
+    };
+
+    const long long vs = (long long)n * nrhs;
+    double* h1 = buf.Hd;
+    double* h2 = buf.Hd + (size_t)(m + 1) * nrhs;
+    double* sq = buf.Hd + (size_t)2 * (m + 1) * nrhs;
+    const size_t hbytes = (size_t)(2 * (m + 1) + 1) * nrhs * 8;
+    std::vector<double> hh((size_t)(2 * (m + 1) + 1) * nrhs);
+    std::vector<double> R((size_t)nrhs * (m + 1) * m, 0.0), g((size_t)nrhs * (m + 1), 0.0),
+        cs((size_t)nrhs * m, 0.0), sn((size_t)nrhs * m, 0.0), beta(nrhs, 0.0),
+        y((size_t)(m + 1) * nrhs, 0.0);
+    double anorm = 0.0;
+    std::vector<double> bnorm(nrhs), rnorm(nrhs), xnorm(nrhs);
+    st = solver.anorm(&anorm);
+    if (st == HDBF_STATUS_SUCCESS) st = solver.host_colmax(B, ldb, bnorm.data());
+    int hinfo = 0;
+    if (st == HDBF_STATUS_SUCCESS) {
+        st = timed(&info.factor_ms, [&] { return solver.factor(prec, &hinfo); });
+        info.factorizations = 1;
+        info.info = hinfo;
+    }
+    if (st == HDBF_STATUS_SUCCESS && hinfo == 0)
+        st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });
+    for (int it = 0; st == HDBF_STATUS_SUCCESS && hinfo == 0; ++it) {
+        st = timed(&info.refine_ms, [&] { return solver.residual(); });
+        if (st != HDBF_STATUS_SUCCESS) break;
+        st = solver.host_colmax(buf.R, n, rnorm.data());
+        if (st == HDBF_STATUS_SUCCESS) st = solver.host_colmax(X, ldx, xnorm.data());
+        if (st != HDBF_STATUS_SUCCESS) break;
+        double berr = 0.0;
+        for (int c = 0; c < nrhs; ++c) {
+            const double den = anorm * xnorm[c] + bnorm[c];
+            const double e = den > 0.0 ? rnorm[c] / den : (rnorm[c] > 0.0 ? INFINITY : 0.0);
+            berr = std::max(berr, std::isfinite(e) ? e : INFINITY);
+        }
+        if (it < HDBF_IR_HISTORY) info.history[it] = berr;
+        info.backward_error = berr;
+        info.iterations = it;
+        if (berr <= tol) {
+            info.converged = 1;
+            break;
+        }
+        if (it >= max_iter) break;
+        // ---- inner GMRES on M^{-1} A d = M^{-1} r
+        int steps = 0;
+        st = timed(&info.refine_ms, [&]() -> hdbf_status {
+            HDBF_TRY(solver.precond(buf.R, n, buf.V, n, false));
+            HDBF_TRY(solver.dots(buf.V, 1, buf.V, sq));
+            HDBF_TRY(solver.normalize(buf.V, sq, buf.V));
+            HDBF_TRY(to_host(hh.data(), buf.Hd, hbytes));
+            std::fill(R.begin(), R.end(), 0.0);
+            std::fill(g.begin(), g.end(), 0.0);
+            for (int c = 0; c < nrhs; ++c) {
+                beta[c] = std::sqrt(hh[(size_t)2 * (m + 1) * nrhs + c]);
+                g[(size_t)c * (m + 1)] = beta[c];
+            }
+            for (int k = 0; k < m; ++k) {
+                double* vk = buf.V + (long long)k * vs;
+                double* vk1 = buf.V + (long long)(k + 1) * vs;
+                HDBF_TRY(solver.matvec(vk, buf.T));
+                HDBF_TRY(solver.precond(buf.T, n, vk1, n, false));
+                HDBF_TRY(solver.dots(buf.V, k + 1, vk1, h1));
+                HDBF_TRY(solver.axpy(buf.V, k + 1, h1, vk1));
+                HDBF_TRY(solver.dots(buf.V, k + 1, vk1, h2));
+                HDBF_TRY(solver.axpy(buf.V, k + 1, h2, vk1));
+                HDBF_TRY(solver.dots(vk1, 1, vk1, sq));
+                HDBF_TRY(solver.normalize(vk1, sq, vk1));
+                HDBF_TRY(to_host(hh.data(), buf.Hd, hbytes));
+                double worst = 0.0;
+                for (int c = 0; c < nrhs; ++c) {
+                    if (!(beta[c] > 0.0)) continue;
+                    double col[64 + 2];
+                    for (int i = 0; i <= k; ++i)
+                        col[i] = hh[(size_t)i * nrhs + c] + hh[(size_t)(m + 1) * nrhs + (size_t)i * nrhs + c];
+                    col[k + 1] = std::sqrt(hh[(size_t)2 * (m + 1) * nrhs + c]);
+                    double* csc = cs.data() + (size_t)c * m;
+                    double* snc = sn.data() + (size_t)c * m;
+                    for (int i = 0; i < k; ++i) {
+                        const double t = csc[i] * col[i] + snc[i] * col[i + 1];
+                        col[i + 1] = -snc[i] * col[i] + csc[i] * col[i + 1];
+                        col[i] = t;
+                    }
+                    const double den = std::hypot(col[k], col[k + 1]);
+                    csc[k] = den > 0.0 ? col[k] / den : 1.0;
+                    snc[k] = den > 0.0 ? col[k + 1] / den : 0.0;
+                    col[k] = den;
+                    double* gc = g.data() + (size_t)c * (m + 1);
+                    gc[k + 1] = -snc[k] * gc[k];
+                    gc[k] = csc[k] * gc[k];
+                    for (int i = 0; i <= k; ++i) R[((size_t)c * (m + 1) + i) * m + k] = col[i];
+                    worst = std::max(worst, std::fabs(gc[k + 1]) / beta[c]);
+                }
+                steps = k + 1;
+                if (worst <= inner_tol) break;
+            }
+            // least squares R y = g per column, then x += V y
+            std::fill(y.begin(), y.end(), 0.0);
+            for (int c = 0; c < nrhs; ++c) {
+                if (!(beta[c] > 0.0)) continue;
+                const double* gc = g.data() + (size_t)c * (m + 1);
+                for (int i = steps - 1; i >= 0; --i) {
+                    double acc = gc[i];
+                    for (int j = i + 1; j < steps; ++j)
+                        acc -= R[((size_t)c * (m + 1) + i) * m + j] * y[(size_t)j * nrhs + c];
+                    const double d = R[((size_t)c * (m + 1) + i) * m + i];
+                    y[(size_t)i * nrhs + c] = d != 0.0 ? acc / d : 0.0;
+                }
+            }
+            if (cudaMemcpyAsync(buf.Yd, y.data(), (size_t)steps * nrhs * 8, cudaMemcpyHostToDevice,
+                                strm) != cudaSuccess)
+                return last_cuda(ctx);
+            return solver.combine(buf.V, steps, buf.Yd);
+        });
+        info.inner_iterations += steps;
+    }
+    info.final_precision = prec;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (out) *out = info;
+    return st;
+}
+
 }  // namespace
 }  // namespace hdbf
 
@@ -505,6 +841,26 @@ hdbf_status hdbf_dgesv_mixed(hdbf_handle h, hdbf_precision prec, int escalate, c
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
     return h->last_status = xsv_mixed(h, false, (int)prec, escalate, A, lda, n, nrhs, B, ldb, X,
                                       ldx, tol, max_iter, out);
+}
+
+hdbf_status hdbf_dposv_mixed_gmres(hdbf_handle h, hdbf_precision prec, const double* A, int lda,
+                                   int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                                   double tol, int max_iter, int max_inner, double inner_tol,
+                                   hdbf_ir_info* out)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = gmres_mixed(h, true, prec, A, lda, n, nrhs, B, ldb, X, ldx, tol,
+                                        max_iter, max_inner, inner_tol, out);
+}
+
+hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle h, hdbf_precision prec, const double* A, int lda,
+                                   int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                                   double tol, int max_iter, int max_inner, double inner_tol,
+                                   hdbf_ir_info* out)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = gmres_mixed(h, false, prec, A, lda, n, nrhs, B, ldb, X, ldx, tol,
+                                        max_iter, max_inner, inner_tol, out);
 }
 
 }  // extern "C"

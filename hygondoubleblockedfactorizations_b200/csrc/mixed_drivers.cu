@@ -208,23 +208,25 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         const int psz = std::min(b, n - k);
         const int tr = n - k - psz;
         float* Akk = at(A, lda, k, k);
-        HDBF_TRY(potrf_diag(ctx, psz, Akk, lda, info, k));
+        const bool inv_tc = trsm_on_tc(pi) && tr > 0 && psz <= potrf_block_max_n();
+        if (inv_tc) HDBF_TRY(potrf_block(ctx, psz, Akk, lda, info, k, wb.W, wb.ldw));
+        else HDBF_TRY(potrf_diag(ctx, psz, Akk, lda, info, k));
         if (tr <= 0) continue;
         float* A21 = at(A, lda, k + psz, k);
-        // L21 = A21 L11^{-T} as one tensor-core GEMM: W = L11^{-T} is the
-        // FP32 TRSM of the identity; A21 is rounded into the shadow and
+        // L21 = A21 L11^{-T} as one tensor-core GEMM with W = L11^{-1} from
+        // the diagonal-block kernel; A21 is rounded into the shadow and
         // overwritten with the product.
-        if (!trsm_on_tc(pi)) {
+        if (!inv_tc) {
             HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
             HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, s));
             HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
                                at(A, lda, k + psz, k + psz), lda, inv_s2, true));
             continue;
         }
-        HDBF_TRY(set_identity(ctx, wb.W, wb.ldw, psz));
-        HDBF_TRY(trsm_rlt(ctx, psz, psz, Akk, lda, wb.W, wb.ldw));
-        HDBF_TRY(convert_direct16(ctx, tp.fmt, psz, psz, wb.W, wb.ldw, wb.wh,
-                                  tp.split ? wb.wl : nullptr, wb.ldws, 1.f));
+        // W = L11^{-1} came with the diagonal factorization; the GEMM's B
+        // operand (N x K, K-major) is W itself, so A21 W^T = A21 L11^{-T}.
+        HDBF_TRY(convert_transpose16(ctx, tp.fmt, psz, psz, wb.W, wb.ldw, wb.wh,
+                                     tp.split ? wb.wl : nullptr, wb.ldws, 1.f));
         HDBF_TRY(convert_transpose16(ctx, tp.fmt, tr, psz, A21, lda, hi,
                                      tp.split ? scratch_lo : nullptr, lds, 1.f));
         HDBF_TRY(zero_block(ctx, A21, lda, tr, psz));

@@ -1,0 +1,372 @@
+// Cholesky of a diagonal block of order n <= 1024 in ONE cooperative launch,
+// optionally with the inverse of its factor.
+//
+// Replaces the reference's rocsolver_spotrf call on the diagonal block
+// (src/potrf/double_blocked_potrf.cpp:34-56, call :334).  The block is cut
+// into 64 x 64 tiles (NT = ceil(n / 64) <= 16) and factored right-looking:
+// for every tile column k one CTA factors the diagonal tile (register-resident
+// potf2) and inverts it, then CTAs solve the tiles below it against that
+// inverse, then CTAs apply the rank-64 update to the trailing tiles -- three
+// phases separated by bounded grid barriers.  With the inverse requested,
+// W = L^{-1} (lower, the strictly upper tiles zeroed) is formed tile diagonal
+// by tile diagonal: W(i,j) = -D_i sum_{m=j}^{i-1} L(i,m) W(m,j), D_i = L(i,i)^{-1}.
+// A recursive factorization of the same block issues ~100 small launches;
+// here the latency chain is 3 NT barriers plus NT tile factorizations.
+//
+// Pivot test and info follow LAPACK xPOTRF: the first column whose updated
+// diagonal is not > 0 (or is NaN) stops the factorization and info =
+// info_base + column + 1 (first failure wins); a block whose info is already
+// non-zero is left untouched.  Every grid-barrier wait is bounded: on expiry
+// the kernel records a timeout, and later barriers return at once.
+#include "internal.h"
+
+namespace hdbf {
+namespace {
+
+constexpr int kT = 64;        // tile
+constexpr int kThreads = 256;
+constexpr int kMaxNT = 16;    // n <= 1024
+constexpr int kLdS = 68;      // padded shared row (float4-aligned)
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+struct Sync {
+    unsigned* ctr;
+    int* fail;
+    int* abort_flag;
+    int* err;
+    unsigned G;
+    unsigned count;  // barriers passed by this CTA
+};
+
+// Grid barrier: arrive (counter += 1 per CTA), wait until all G CTAs of this
+// round arrived.  Bounded; once any CTA gave up, later waits return at once.
+__device__ void grid_barrier(Sync& s)
+{
+    __syncthreads();
+    s.count += 1;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(s.ctr, 1u);
+        const unsigned target = s.count * s.G;
+        unsigned polls = 0;
+        while (ld_acquire_u32(s.ctr) < target) {
+            if (*reinterpret_cast<volatile int*>(s.abort_flag)) break;
+            if (++polls > kSpinLimit) {
+                atomicExch(s.err, kErrTimeout);
+                atomicExch(s.abort_flag, 1);
+                break;
+            }
+            if (polls > 64) __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// dst[k][m] = src(m, k) = src[k * ld + m] (column-major 64 x 64 tile, k-major
+// in shared memory); entries outside rows x cols are zero.
+__device__ __forceinline__ void load_kmajor(float* dst, const float* src, long long ld, int rows,
+                                            int cols)
+{
+    for (int q = threadIdx.x; q < kT * kT; q += kThreads) {
+        const int k = q >> 6, m = q & 63;
+        dst[k * kLdS + m] = (m < rows && k < cols) ? __ldcg(src + (long long)k * ld + m) : 0.f;
+    }
+}
+
+// dst[k][n] = src(k, n) = src[n * ld + k] (transposing load).
+__device__ __forceinline__ void load_trans(float* dst, const float* src, long long ld, int rows,
+                                           int cols)
+{
+    for (int q = threadIdx.x; q < kT * kT; q += kThreads) {
+        const int n = q >> 6, k = q & 63;
+        dst[k * kLdS + n] = (k < rows && n < cols) ? __ldcg(src + (long long)n * ld + k) : 0.f;
+    }
+}
+
+// acc[i][j] += sum_k As[k][ty*4+i] * Bs[k][tx*4+j]
+__device__ __forceinline__ void tile_mma(float acc[4][4], const float* As, const float* Bs)
+{
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll 8
+    for (int k = 0; k < kT; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(As + k * kLdS + ty * 4);
+        const float4 b = *reinterpret_cast<const float4*>(Bs + k * kLdS + tx * 4);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+        const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+}
+
+// Register-resident Cholesky of the nb x nb (nb <= 64) lower tile at T
+// (thread (r, g) holds T(r, g + 4i), i < 16).  Returns the first failing
+// column or -1 (uniform over the CTA).
+__device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_d)
+{
+    const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
+    float a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = g + 4 * i;
+        a[i] = (r < nb && c < nb && r >= c) ? __ldcg(T + (long long)c * ld + r) : 0.f;
+    }
+    int failed_at = -1;
+    for (int j = 0; j < nb; ++j) {
+        const int gj = j & 3, ij = j >> 2;
+        float own = 0.f;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (i == ij) own = a[i];
+        if (g == gj && r == j) *s_d = own;
+        __syncthreads();
+        const float d = *s_d;
+        if (!(d > 0.f)) {
+            failed_at = j;
+            break;
+        }
+        const float sd = sqrtf(d);
+        const float rcp = 1.0f / sd;
+        if (g == gj) {
+            const float v = (r == j) ? sd : (r > j ? own * rcp : own);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (i == ij) a[i] = v;
+            if (r > j) lcol[r] = v;
+        }
+        __syncthreads();
+        if (r > j) {
+            const float lr = lcol[r];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int c = g + 4 * i;
+                if (c > j && c <= r) a[i] = fmaf(-lr, lcol[c], a[i]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = g + 4 * i;
+        if (r < nb && c < nb && r >= c) T[(long long)c * ld + r] = a[i];
+    }
+    return failed_at;
+}
+
+// D = L^{-1} for the nb x nb lower tile L (padded with the identity to 64):
+// thread t < 64 solves L x = e_t by forward substitution over a shared copy.
+// D is written column-major with leading dimension 64 (D[c * 64 + r]).
+__device__ void tri_inv_tile(const float* L, long long ld, int nb, float* Ls /*64 x 65*/,
+                             float* D)
+{
+    for (int q = threadIdx.x; q < kT * kT; q += kThreads) {
+        const int c = q >> 6, r = q & 63;
+        Ls[r * 65 + c] = (r < nb && c < nb && r >= c) ? __ldcg(L + (long long)c * ld + r) : 0.f;
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < kT) {
+        float x[kT];
+#pragma unroll
+        for (int i = 0; i < kT; ++i) x[i] = (i == t) ? 1.f : 0.f;
+#pragma unroll
+        for (int k = 0; k < kT; ++k) {
+            if (k < nb) {
+                x[k] = x[k] / Ls[k * 65 + k];
+#pragma unroll
+                for (int i = k + 1; i < kT; ++i) x[i] = fmaf(-Ls[i * 65 + k], x[k], x[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kT; ++i) D[t * kT + i] = x[i];  // column t
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, float* W,
+                   long long ldw, float* dinv, unsigned* ctr, int* fail, int* abort_flag, int* err)
+{
+    __shared__ __align__(16) float As[kT * kLdS];
+    __shared__ __align__(16) float Bs[kT * kLdS];
+    __shared__ float lcol[kT];
+    __shared__ float s_d;
+    __shared__ int s_flag;
+    const int NT = (n + kT - 1) / kT;
+    const int cta = blockIdx.x;
+    const unsigned G = gridDim.x;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    Sync sy{ctr, fail, abort_flag, err, G, 0u};
+    auto tile = [&](int i, int j) { return A + (long long)(j * kT) * lda + i * kT; };
+    auto ext = [&](int i) { return min(kT, n - i * kT); };
+
+    if (tid == 0) s_flag = (info && *reinterpret_cast<volatile int*>(info) != 0) ? 1 : 0;
+    __syncthreads();
+    const bool skip = s_flag != 0;  // same value in every CTA: read before any write
+    grid_barrier(sy);
+    if (skip) return;
+
+    bool ok = true;
+    for (int k = 0; k < NT && ok; ++k) {
+        // P1: factor and invert the diagonal tile
+        if (cta == 0) {
+            const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d);
+            if (f >= 0) {
+                if (tid == 0) {
+                    if (info) atomicCAS(info, 0, info_base + k * kT + f + 1);
+                    atomicExch(fail, 1);
+                }
+            } else {
+                __syncthreads();
+                tri_inv_tile(tile(k, k), lda, ext(k), As, dinv + (long long)k * kT * kT);
+            }
+        }
+        grid_barrier(sy);
+        if (tid == 0) s_flag = *reinterpret_cast<volatile int*>(fail) |
+                               *reinterpret_cast<volatile int*>(abort_flag);
+        __syncthreads();
+        if (s_flag) { ok = false; break; }
+        if (k == NT - 1) break;
+        // P2: L(i,k) = A(i,k) D_k^T for i > k
+        for (int i = k + 1 + cta; i < NT; i += G) {
+            load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
+            load_kmajor(Bs, dinv + (long long)k * kT * kT, kT, ext(k), ext(k));
+            __syncthreads();
+            float acc[4][4] = {};
+            tile_mma(acc, As, Bs);
+            float* T = tile(i, k);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int r = ty * 4 + a, c = tx * 4 + b;
+                    if (r < ext(i) && c < ext(k)) T[(long long)c * lda + r] = acc[a][b];
+                }
+            __syncthreads();
+        }
+        grid_barrier(sy);
+        // P3: A(i,j) -= L(i,k) L(j,k)^T for k < j <= i
+        const int rem = NT - 1 - k;
+        const int pairs = rem * (rem + 1) / 2;
+        for (int t = cta; t < pairs; t += G) {
+            int i = k + 1, j = k + 1, left = t;
+            while (left > i - (k + 1)) { left -= i - k; ++i; }
+            j = k + 1 + left;
+            load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
+            load_kmajor(Bs, tile(j, k), lda, ext(j), ext(k));
+            __syncthreads();
+            float acc[4][4] = {};
+            tile_mma(acc, As, Bs);
+            float* T = tile(i, j);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int r = ty * 4 + a, c = tx * 4 + b;
+                    if (r < ext(i) && c < ext(j) && (i != j || r >= c)) {
+                        const long long o = (long long)c * lda + r;
+                        T[o] = __ldcg(T + o) - acc[a][b];
+                    }
+                }
+            __syncthreads();
+        }
+        grid_barrier(sy);
+    }
+    if (!ok || !W) return;
+
+    // W = L^{-1}: diagonal tiles D_i, strictly upper tiles zero
+    for (int t = cta; t < NT * NT; t += G) {
+        const int i = t % NT, j = t / NT;
+        if (i < j) {
+            for (int q = tid; q < kT * kT; q += kThreads) {
+                const int c = q >> 6, r = q & 63;
+                if (r < ext(i) && c < ext(j)) W[(long long)(j * kT + c) * ldw + i * kT + r] = 0.f;
+            }
+        } else if (i == j) {
+            const float* D = dinv + (long long)i * kT * kT;
+            for (int q = tid; q < kT * kT; q += kThreads) {
+                const int c = q >> 6, r = q & 63;
+                if (r < ext(i) && c < ext(i))
+                    W[(long long)(i * kT + c) * ldw + i * kT + r] = __ldcg(D + c * kT + r);
+            }
+        }
+    }
+    grid_barrier(sy);
+    for (int d = 1; d < NT; ++d) {
+        for (int i = d + cta; i < NT; i += G) {
+            const int j = i - d;
+            float acc[4][4] = {};
+            for (int m = j; m < i; ++m) {
+                load_kmajor(As, tile(i, m), lda, ext(i), ext(m));
+                load_trans(Bs, W + (long long)(j * kT) * ldw + m * kT, ldw, ext(m), ext(j));
+                __syncthreads();
+                tile_mma(acc, As, Bs);
+                __syncthreads();
+            }
+            // W(i,j) = -D_i acc
+            load_kmajor(As, dinv + (long long)i * kT * kT, kT, ext(i), ext(i));
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) Bs[(ty * 4 + a) * kLdS + tx * 4 + b] = acc[a][b];
+            __syncthreads();
+            float w[4][4] = {};
+            tile_mma(w, As, Bs);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int r = ty * 4 + a, c = tx * 4 + b;
+                    if (r < ext(i) && c < ext(j))
+                        W[(long long)(j * kT + c) * ldw + i * kT + r] = -w[a][b];
+                }
+            __syncthreads();
+        }
+        grid_barrier(sy);
+    }
+}
+
+}  // namespace
+
+int potrf_block_max_n() { return kT * kMaxNT; }
+
+hdbf_status potrf_block(hdbf_context* ctx, int n, float* A, long long lda, int* info,
+                        int info_base, float* W, long long ldw)
+{
+    if (n <= 0) return HDBF_STATUS_SUCCESS;
+    if (n > kT * kMaxNT || lda < n || (W && ldw < n)) return HDBF_STATUS_INVALID_VALUE;
+    HDBF_TRY(ensure_ws(ctx, n));
+    const int NT = (n + kT - 1) / kT;
+    int G = NT * (NT - 1) / 2;
+    if (W && NT * NT > G) G = NT * NT;  // the W set-up pass touches NT^2 tiles
+    if (G > ctx->sm_count) G = ctx->sm_count;
+    if (G < 1) G = 1;
+    int* sm = ctx->dev_small + kSmallBlockBar;
+    if (cudaMemsetAsync(sm, 0, 3 * sizeof(int), ctx->stream) != cudaSuccess) return last_cuda(ctx);
+    unsigned* ctr = reinterpret_cast<unsigned*>(sm);
+    int* fail = sm + 1;
+    int* abort_flag = sm + 2;
+    int* err = ctx->dev_small + kSmallErr;
+    float* dinv = ws_inv(ctx);
+    const double flops = (double)n * n * n / 3.0 + (W ? (double)n * n * n / 3.0 : 0.0);
+    ProfScope prof(ctx, kClsPotrfBlock, flops, 8.0 * n * n, n, n, n);
+    void* args[] = {&n, &A, &lda, &info, &info_base, &W, &ldw, &dinv, &ctr, &fail, &abort_flag,
+                    &err};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)potrf_block_kernel, dim3(G),
+                                                      dim3(kThreads), args, 0, ctx->stream);
+    ctx->launches++;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
+}  // namespace hdbf

@@ -557,7 +557,7 @@ const char* hdbf_profile_class_name(int cls)
                                              "ir_fp64_kernels", "other",
                                              "trsv_wave_kernel", "sgemm_skinny_kernel",
                                              "batched_factor_solve_kernel",
-                                             "selector_mlp_kernels"};
+                                             "selector_mlp_kernels", "potrf_block_kernel"};
     return (cls >= 0 && cls < kNumClasses) ? names[cls] : "unknown";
 }
 

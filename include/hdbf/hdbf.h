@@ -94,7 +94,7 @@ hdbf_status hdbf_set_graph_mode(hdbf_handle handle, int enabled);
  * The panel recursion stops at leaves of 128 columns (the grid-wide kernel
  * takes up to 128; the cluster kernel up to 32, so mode 2 recurses to 32);
  * HDBF_PANEL_LEAF (32, 64 or 128) sets a new handle's leaf width, and
- * HDBF_PANEL_ROWS (64..4096, default 512) the rows each CTA of the grid-wide
+ * HDBF_PANEL_ROWS (64..4096, default 256) the rows each CTA of the grid-wide
  * kernel aims to hold. */
 hdbf_status hdbf_set_panel_kernel(hdbf_handle handle, int mode);
 

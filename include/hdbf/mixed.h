@@ -51,6 +51,7 @@ typedef struct hdbf_ir_info {
     double history[HDBF_IR_HISTORY]; /* backward error after each step (history[0] = initial) */
     double factor_ms;         /* device time of the factorizations */
     double refine_ms;         /* device time of solves + residuals + updates */
+    int inner_iterations;     /* GMRES-IR: preconditioned GMRES steps over all outer steps */
 } hdbf_ir_info;
 
 /* Solve A X = B (A SPD for posv, general for gesv; A, B, X FP64).  The FP64 A
@@ -65,6 +66,22 @@ hdbf_status hdbf_dposv_mixed(hdbf_handle handle, hdbf_precision prec, int escala
 hdbf_status hdbf_dgesv_mixed(hdbf_handle handle, hdbf_precision prec, int escalate,
                              const double* A, int lda, int n, int nrhs, const double* B, int ldb,
                              double* X, int ldx, double tol, int max_iter, hdbf_ir_info* out);
+
+/* GMRES-IR (Carson-Higham): the same factorizations, but each correction
+ * solves A d = r with restarted GMRES in FP64 (at most max_inner steps, CGS2
+ * orthogonalisation, all right-hand sides in lockstep) preconditioned from the
+ * left by the low-precision factors, until the preconditioned residual falls
+ * by inner_tol.  Converges where classical refinement stalls (BF16/FP16 LU of
+ * large n, or kappa * u_factor near or above 1).  Outer steps stop at tol or
+ * max_iter; no escalation.  nrhs <= 64. */
+hdbf_status hdbf_dposv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, const double* A,
+                                   int lda, int n, int nrhs, const double* B, int ldb, double* X,
+                                   int ldx, double tol, int max_iter, int max_inner,
+                                   double inner_tol, hdbf_ir_info* out);
+hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, const double* A,
+                                   int lda, int n, int nrhs, const double* B, int ldb, double* X,
+                                   int ldx, double tol, int max_iter, int max_inner,
+                                   double inner_tol, hdbf_ir_info* out);
 
 #ifdef __cplusplus
 }

@@ -127,6 +127,47 @@ def test_dgesv_mixed_ir(hd, handle, torch_cuda, kappa, prec):
     assert oracle.backward_error(A, X, B) <= 1e-13
 
 
+def run_gmres(hd, handle, torch, fn, A, B, prec, tol=1e-13, max_iter=10, max_inner=30,
+              inner_tol=1e-4):
+    n, nrhs = B.shape
+    dA, dB = dev(torch, A), dev(torch, B)
+    dX = torch.zeros(n * nrhs, dtype=torch.float64, device="cuda")
+    info = hd_mod.IrInfo()
+    st = hd.call(fn, handle.ptr, hd_mod.PREC[prec], ptr(dA), n, n, nrhs, ptr(dB), n, ptr(dX), n,
+                 tol, max_iter, max_inner, inner_tol, ctypes.byref(info))
+    torch.cuda.synchronize()
+    return st, host2d(dX, n, n, nrhs), info
+
+
+# GMRES-IR: FP64 GMRES preconditioned by the low-precision factors converges
+# to the FP64 backward-error target where classical refinement needs
+# escalation (BF16 LU) or stalls (kappa = 1e6 with FP32 factors), within the
+# method's range kappa * u_factor <~ 1 (FP16 reaches kappa ~ 1e4, the split
+# modes and FP32 kappa ~ 1e6).
+@pytest.mark.parametrize("kappa,prec", [(1e2, "bf16"), (1e2, "fp16"), (1e4, "fp16"),
+                                        (1e6, "fp16x3"), (1e6, "fp32")])
+def test_dgesv_mixed_gmres(hd, handle, torch_cuda, kappa, prec):
+    n, nrhs = 1024, 16
+    A = oracle.general_kappa(n, kappa, 21)
+    B = np.random.default_rng(22).standard_normal((n, nrhs))
+    st, X, info = run_gmres(hd, handle, torch_cuda, "hdbf_dgesv_mixed_gmres", A, B, prec)
+    assert st == 0, hd_mod.status_string(st)
+    assert info.converged == 1, (info.backward_error, list(info.history[:info.iterations + 1]))
+    assert oracle.backward_error(A, X, B) <= 1e-13
+    assert info.inner_iterations >= 1 and info.factorizations == 1
+
+
+@pytest.mark.parametrize("kappa,prec", [(1e2, "bf16"), (1e4, "fp16"), (1e6, "fp16x3")])
+def test_dposv_mixed_gmres(hd, handle, torch_cuda, kappa, prec):
+    n, nrhs = 1024, 5
+    A = oracle.spd_kappa(n, kappa, 11)
+    B = np.random.default_rng(12).standard_normal((n, nrhs))
+    st, X, info = run_gmres(hd, handle, torch_cuda, "hdbf_dposv_mixed_gmres", A, B, prec)
+    assert st == 0, hd_mod.status_string(st)
+    assert info.converged == 1, (info.backward_error, list(info.history[:info.iterations + 1]))
+    assert oracle.backward_error(A, X, B) <= 1e-13
+
+
 def test_recursive_potrf_mixed_driver(hd, handle, torch_cuda):
     n = 1024
     A = oracle.spd_gram(n, 5)

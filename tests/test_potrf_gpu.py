@@ -74,7 +74,8 @@ def test_config0_all_variants(hd, handle, torch_cuda, fn, kw):
 
 @pytest.mark.parametrize("n,nb,b", [(1, 0, 0), (2, 1, 1), (3, 2, 1), (17, 8, 3), (63, 64, 64),
                                     (64, 32, 16), (65, 64, 64), (127, 50, 7), (130, 128, 64),
-                                    (257, 100, 33), (500, 256, 96), (1000, 384, 128)])
+                                    (257, 100, 33), (500, 256, 96), (1000, 384, 128),
+                                    (700, 700, 700), (1000, 1000, 1000), (1100, 1024, 1024)])
 def test_ragged_sizes_padding_and_upper_untouched(hd, handle, torch_cuda, n, nb, b):
     A = oracle.spd_gram(n, 11)
     lda = n + 5
@@ -106,6 +107,21 @@ def test_not_positive_definite_info(hd, handle, torch_cuda, fail_at):
     for fn in ("double_blocked_potrf", "recursive_potrf", "blocked_right_looking_potrf"):
         _, info = run_potrf(hd, handle, torch_cuda, A, fn, nb=256, b=64)
         assert info == linfo == fail_at + 1, fn
+
+
+@pytest.mark.parametrize("fail_at", [0, 63, 64, 300, 1000])
+@pytest.mark.parametrize("b", [512, 1024])
+def test_not_positive_definite_info_block_kernel(hd, handle, torch_cuda, fail_at, b):
+    """Diagonal blocks of 65..1024 are factored by one cooperative launch;
+    its info must still be the first non-positive leading minor."""
+    n = 1024
+    A = oracle.spd_gram(n, 3).astype(np.float64)
+    A[fail_at, fail_at] = -50.0
+    A = A.astype(np.float32)
+    _, linfo = oracle.lapack_spotrf(A)
+    _, info = run_potrf(hd, handle, torch_cuda, A, "double_blocked_potrf", nb=b, b=b)
+    assert info == linfo == fail_at + 1
+    assert handle.device_errors() == 0
 
 
 def test_zero_order_and_invalid_arguments(hd, handle, torch_cuda):
