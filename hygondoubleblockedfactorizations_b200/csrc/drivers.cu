@@ -43,6 +43,7 @@ hdbf_status trsm_rlt_rec(hdbf_context* ctx, int rows, int cols, const float* L, 
                          float* B, long long ldb, const float* inv)
 {
     if (cols <= kDiagLeaf) return rlt_apply(ctx, rows, cols, inv, B, ldb);
+    if (cols <= llu_block_max_rows()) return rlt_block(ctx, rows, cols, L, ldl, inv, B, ldb);
     const int c1 = split_at(cols, kDiagLeaf);
     const int c2 = cols - c1;
     HDBF_TRY(trsm_rlt_rec(ctx, rows, c1, L, ldl, B, ldb, inv));
@@ -57,6 +58,7 @@ hdbf_status trsm_llu_rec(hdbf_context* ctx, int rows, int cols, const float* L, 
                          float* B, long long ldb, const float* inv)
 {
     if (rows <= kDiagLeaf) return llu_apply(ctx, rows, cols, inv, B, ldb);
+    if (rows <= llu_block_max_rows()) return llu_block(ctx, rows, cols, L, ldl, inv, B, ldb);
     const int r1 = split_at(rows, kDiagLeaf);
     const int r2 = rows - r1;
     HDBF_TRY(trsm_llu_rec(ctx, r1, cols, L, ldl, B, ldb, inv));

@@ -187,6 +187,15 @@ hdbf_status rlt_apply(hdbf_context* ctx, int rows, int cols, const float* inv, f
 // Inverse modes: 0 lower non-unit, 1 lower unit, 2 upper non-unit.
 hdbf_status tri_inv64_mode(hdbf_context* ctx, int n, const float* L, long long ldl, int mode,
                            float* out);
+// B(rows <= 256 x cols) <- L^{-1} B for unit lower L in one launch (block
+// forward substitution with the 64x64 inverses in inv, trsm_block.cu).
+hdbf_status llu_block(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
+                      const float* inv, float* B, long long ldb);
+int llu_block_max_rows();
+// B(rows x cols <= 256) <- B L^{-T}, L lower non-unit, same scheme.
+hdbf_status rlt_block(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
+                      const float* inv, float* B, long long ldb);
+void configure_trsm_block_kernels(hdbf_context* ctx);
 // B <- inv * B (trans=false) or inv^T * B (trans=true), rows <= 64.
 hdbf_status llu_apply_t(hdbf_context* ctx, int rows, int cols, const float* inv, float* B,
                         long long ldb, bool trans);

@@ -344,6 +344,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
         if (v >= 64 && v <= 4096) ctx->panel_rows = v;
     }
     configure_tc_kernels(ctx);
+    configure_trsm_block_kernels(ctx);
     configure_solve_kernels(ctx);
     configure_batched_kernels(ctx);
     const int one = 1;  // exchange epoch starts at 1: zeroed slots never match
