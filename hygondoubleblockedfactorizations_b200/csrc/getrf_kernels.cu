@@ -163,10 +163,9 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
             slot[2] = __int_as_float(my_best);
         }
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_release_u32(reinterpret_cast<unsigned*>(slot), seq);
-        }
+        // The release store (after the barrier) orders every thread's slot
+        // writes before the sequence number that other CTAs acquire.
+        if (tid == 0) st_release_u32(reinterpret_cast<unsigned*>(slot), seq);
 
         // 3. poll every slot (thread q watches CTA q), bounded
         for (int q = tid; q < G; q += kCoopThreads) {

@@ -111,8 +111,10 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
         }
     };
 
-    const int tx = tid & 15;
-    const int ty = tid >> 4;
+    // 16 x 16 thread tiles; each warp covers 8 (ty) x 4 (tx) of them, so a
+    // k-step's A and B fragment reads are one shared-memory wavefront each.
+    const int tx = ((tid >> 5) & 3) * 4 + (tid & 3);
+    const int ty = (tid >> 7) * 8 + ((tid & 31) >> 2);
 
     float acc[8][8];
 #pragma unroll

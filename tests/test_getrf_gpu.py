@@ -227,24 +227,38 @@ def test_graph_replay_getrf(hd, handle, torch_cuda):
 
 
 def test_panel_kernels_agree_bitwise_large(hd, handle, torch_cuda):
-    """n = 16384: the first panels run on 16-CTA clusters, later ones on 8, 4,
-    2 and 1; the grid-wide kernel must give bit-identical factors and pivots
-    (same arithmetic, same order).  Pivots follow host sgetrf up to FP32
+    """n = 16384 with 32-column leaves: the first panels run on 16-CTA clusters,
+    later ones on 8, 4, 2 and 1; the grid-wide kernel must give bit-identical
+    factors and pivots (same arithmetic, same order).  Pivots follow host sgetrf up to FP32
     near-ties; the residual is the FP64 ||PA - LU||_F / ||A||_F (GPU FP64,
     same formula as the oracle), scaled by n * eps32."""
+    import os
     n = 16384
     G = oracle.general_uniform(n, 1)
     out = {}
-    for panel in (0, 1):
-        handle.set_panel_kernel(panel)
-        dA, _, ipiv, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf",
+    os.environ["HDBF_PANEL_LEAF"] = "32"  # same recursion for both kernels
+    try:
+        h32 = hd.Handle(torch_cuda.cuda.current_stream().cuda_stream)
+    finally:
+        del os.environ["HDBF_PANEL_LEAF"]
+    for panel in (2, 1):  # 2: cluster kernel, 1: grid-wide kernel
+        h32.set_panel_kernel(panel)
+        dA, _, ipiv, info = run_getrf(hd, h32, torch_cuda, G, "double_blocked_getrf",
                                       outer=4096, inner=512)
-        assert info == 0 and handle.device_errors() == 0
+        assert info == 0 and h32.device_errors() == 0
         out[panel] = (dA.clone(), ipiv)
+    h32.close()
+    out[0] = out[2]
+    # the default (128-column leaves) must also follow host sgetrf
+    _, _, ipiv128, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf",
+                                    outer=4096, inner=512)
+    assert info == 0
+    lapack_piv = oracle.lapack_sgetrf(G)[1]
+    assert_pivots_match(G, ipiv128, lapack_piv, "host sgetrf (leaf 128)")
     assert np.array_equal(out[0][1], out[1][1])
     assert torch_cuda.equal(out[0][0], out[1][0])
     ipiv = out[0][1]
-    assert_pivots_match(G, ipiv, oracle.lapack_sgetrf(G)[1], "host sgetrf")
+    assert_pivots_match(G, ipiv, lapack_piv, "host sgetrf")
     torch = torch_cuda
     LU = out[0][0].view(n, n).t().double()  # row-major view of the column-major factor
     L = torch.tril(LU, -1) + torch.eye(n, dtype=torch.float64, device="cuda")
