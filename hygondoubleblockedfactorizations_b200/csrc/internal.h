@@ -256,6 +256,11 @@ constexpr int kFmtBF16 = 1;  // bfloat16
 // C(M x N, FP32 column-major) -= scale * A * B^T on the tensor cores.
 hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
                         const TcOperand& B, float* C, long long ldc, float scale, bool lower_only);
+// C -= scale * (A B^T + A Blo^T + Alo B^T): the split-precision product in one
+// launch (hi/lo operands share row/K origins), one FP32 accumulator in TMEM.
+hdbf_status tc_gemm_sub_split(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
+                              const TcOperand& Alo, const TcOperand& B, const TcOperand& Blo,
+                              float* C, long long ldc, float scale, bool lower_only);
 void configure_tc_kernels(hdbf_context* ctx);
 // dst(r, k) = round16(s * src(r, k)) for an rows x cols FP32 column-major block
 // into a K-major (row-major, ldd elements) 16-bit block; `hi_lo` additionally

@@ -65,13 +65,11 @@ hdbf_status tc_update(hdbf_context* ctx, const PrecInfo& pi, int M, int N, int K
     a.ld = lda;
     b.base = bh;
     b.ld = ldb;
-    HDBF_TRY(tc_gemm_sub(ctx, pi.fmt, M, N, K, a, b, C, ldc, scale, lower));
-    if (!pi.split) return HDBF_STATUS_SUCCESS;
+    if (!pi.split) return tc_gemm_sub(ctx, pi.fmt, M, N, K, a, b, C, ldc, scale, lower);
     TcOperand alo = a, blo = b;
     alo.base = al;
     blo.base = bl;
-    HDBF_TRY(tc_gemm_sub(ctx, pi.fmt, M, N, K, a, blo, C, ldc, scale, lower));
-    return tc_gemm_sub(ctx, pi.fmt, M, N, K, alo, b, C, ldc, scale, lower);
+    return tc_gemm_sub_split(ctx, pi.fmt, M, N, K, a, alo, b, blo, C, ldc, scale, lower);
 }
 
 __global__ void absmax_kernel(const float* A, long long lda, int rows, int cols, int diag_only,

@@ -31,12 +31,19 @@ namespace {
 constexpr int TM = 128;
 constexpr int TN = 128;
 constexpr int TK = 64;  // 64 x 16-bit = 128 bytes = one swizzle row
-constexpr int STAGES = 3;  // 2 CTAs per SM: one's epilogue overlaps the other's main loop
 constexpr int A_BYTES = TM * TK * 2;
 constexpr int B_BYTES = TN * TK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 128;
-constexpr size_t kTcSmem = (size_t)STAGES * STAGE_BYTES + 1024;  // + alignment slack
+// One product: 3 stages of (A, B), 2 CTAs per SM (one's epilogue overlaps the
+// other's main loop).  Split (hi/lo) operands: 2 stages of (A, B, A_lo, B_lo)
+// and the three products hi*hi + hi*lo + lo*hi into one accumulator, 1 CTA/SM.
+template <bool SPLIT>
+struct TcCfg {
+    static constexpr int kStages = SPLIT ? 2 : 3;
+    static constexpr int kStageBytes = SPLIT ? 2 * STAGE_BYTES : STAGE_BYTES;
+    static constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024;  // + alignment slack
+};
 constexpr long long kWaitCycles = 4000000000LL;                   // ~2 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -120,10 +127,14 @@ struct TcArgs {
     int* err;
 };
 
-__global__ void __launch_bounds__(128, 2)
+template <bool SPLIT>
+__global__ void __launch_bounds__(128, SPLIT ? 1 : 2)
 tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                   const TcArgs args)
+                   const __grid_constant__ CUtensorMap mapAl,
+                   const __grid_constant__ CUtensorMap mapBl, const TcArgs args)
 {
+    constexpr int STAGES = TcCfg<SPLIT>::kStages;
+    constexpr int SB = TcCfg<SPLIT>::kStageBytes;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES];
     __shared__ __align__(8) uint64_t empty_bar[STAGES];
@@ -138,8 +149,11 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
 
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                ~static_cast<uintptr_t>(1023));
-    uint8_t* sA = smem;
-    uint8_t* sB = smem + STAGES * A_BYTES;
+    // stage s: [A | B | A_lo | B_lo] (each tile 1024-byte aligned)
+    auto sA = [&](int st) { return smem + st * SB; };
+    auto sB = [&](int st) { return smem + st * SB + A_BYTES; };
+    auto sAl = [&](int st) { return smem + st * SB + STAGE_BYTES; };
+    auto sBl = [&](int st) { return smem + st * SB + STAGE_BYTES + A_BYTES; };
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (warp == 0) {
@@ -171,9 +185,13 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
                 s_fail = 1;
                 break;
             }
-            mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-            tma_load_2d(sA + s * A_BYTES, &mapA, &full_bar[s], args.a_k0 + kt * TK, args.a_row0 + m0);
-            tma_load_2d(sB + s * B_BYTES, &mapB, &full_bar[s], args.b_k0 + kt * TK, args.b_row0 + n0);
+            mbar_expect_tx(&full_bar[s], SB);
+            tma_load_2d(sA(s), &mapA, &full_bar[s], args.a_k0 + kt * TK, args.a_row0 + m0);
+            tma_load_2d(sB(s), &mapB, &full_bar[s], args.b_k0 + kt * TK, args.b_row0 + n0);
+            if (SPLIT) {
+                tma_load_2d(sAl(s), &mapAl, &full_bar[s], args.a_k0 + kt * TK, args.a_row0 + m0);
+                tma_load_2d(sBl(s), &mapBl, &full_bar[s], args.b_k0 + kt * TK, args.b_row0 + n0);
+            }
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
@@ -185,18 +203,26 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t a0 = smem_u32(sA + s * A_BYTES);
-            const uint32_t b0 = smem_u32(sB + s * B_BYTES);
-#pragma unroll
-            for (int kk = 0; kk < TK / 16; ++kk) {
-                const uint64_t ad = sw128_desc(a0 + kk * 32);
-                const uint64_t bd = sw128_desc(b0 + kk * 32);
-                const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+            const uint32_t a0 = smem_u32(sA(s));
+            const uint32_t b0 = smem_u32(sB(s));
+            const uint32_t al0 = smem_u32(sAl(s));
+            const uint32_t bl0 = smem_u32(sBl(s));
+            auto mma = [&](uint64_t ad, uint64_t bd, uint32_t acc) {
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(taddr),
                     "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            };
+#pragma unroll
+            for (int kk = 0; kk < TK / 16; ++kk) {
+                const uint64_t ad = sw128_desc(a0 + kk * 32);
+                const uint64_t bd = sw128_desc(b0 + kk * 32);
+                mma(ad, bd, (kt > 0 || kk > 0) ? 1u : 0u);
+                if (SPLIT) {
+                    mma(ad, sw128_desc(bl0 + kk * 32), 1u);
+                    mma(sw128_desc(al0 + kk * 32), bd, 1u);
+                }
             }
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -309,25 +335,43 @@ bool make_map(CUtensorMap* map, const void* base, long long ld, long long row_ex
 void configure_tc_kernels(hdbf_context* ctx)
 {
     (void)ctx;
-    cudaFuncSetAttribute(tc_gemm_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kTcSmem);
+    cudaFuncSetAttribute(tc_gemm_sub_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TcCfg<false>::kSmem);
+    cudaFuncSetAttribute(tc_gemm_sub_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TcCfg<true>::kSmem);
     cudaGetLastError();
 }
 
-hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
-                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only)
+namespace {
+hdbf_status tc_launch(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
+                      const TcOperand& B, const TcOperand* Alo, const TcOperand* Blo, float* C,
+                      long long ldc, float scale, bool lower_only)
 {
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
-    if (!A.base || !B.base || !C) return HDBF_STATUS_INVALID_VALUE;
-    // TMA: 16-byte aligned base and row stride; the K coordinate of every
-    // tile must start on a 16-byte (8-element) boundary.
-    if ((reinterpret_cast<uintptr_t>(A.base) & 15u) || (reinterpret_cast<uintptr_t>(B.base) & 15u) ||
-        (A.ld % 8) || (B.ld % 8) || (A.k0 % 8) || (B.k0 % 8))
+    const bool split = Alo && Blo;
+    const TcOperand* ops[4] = {&A, &B, Alo, Blo};
+    for (int q = 0; q < (split ? 4 : 2); ++q) {
+        const TcOperand& o = *ops[q];
+        // TMA: 16-byte aligned base and row stride; the K coordinate of every
+        // tile must start on a 16-byte (8-element) boundary.
+        if (!o.base || (reinterpret_cast<uintptr_t>(o.base) & 15u) || (o.ld % 8) || (o.k0 % 8))
+            return HDBF_STATUS_INVALID_VALUE;
+    }
+    if (!C) return HDBF_STATUS_INVALID_VALUE;
+    if (split && (Alo->row0 != A.row0 || Alo->k0 != A.k0 || Blo->row0 != B.row0 || Blo->k0 != B.k0))
         return HDBF_STATUS_INVALID_VALUE;
-    CUtensorMap ma, mb;
+    CUtensorMap ma, mb, mal, mbl;
     if (!make_map(&ma, A.base, A.ld, (long long)A.row0 + M, (long long)A.k0 + K, fmt) ||
         !make_map(&mb, B.base, B.ld, (long long)B.row0 + N, (long long)B.k0 + K, fmt))
         return HDBF_STATUS_NOT_SUPPORTED;
+    if (split) {
+        if (!make_map(&mal, Alo->base, Alo->ld, (long long)A.row0 + M, (long long)A.k0 + K, fmt) ||
+            !make_map(&mbl, Blo->base, Blo->ld, (long long)B.row0 + N, (long long)B.k0 + K, fmt))
+            return HDBF_STATUS_NOT_SUPPORTED;
+    } else {
+        mal = ma;
+        mbl = mb;
+    }
     TcArgs args;
     args.M = M;
     args.N = N;
@@ -345,12 +389,31 @@ hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const T
     args.err = ctx->dev_small + kSmallErr;
     const long long grid = (long long)args.tiles_m * ((N + TN - 1) / TN);
     if (grid > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
-    double flops = 2.0 * (double)M * N * K;
-    ProfScope prof(ctx, kClsTcGemm, flops, 2.0 * ((double)M * K + (double)N * K) + 8.0 * M * N, M,
-                   N, K);
-    tc_gemm_sub_kernel<<<(unsigned)grid, 128, kTcSmem, ctx->stream>>>(ma, mb, args);
+    const double flops = (split ? 3.0 : 1.0) * 2.0 * (double)M * N * K;
+    ProfScope prof(ctx, kClsTcGemm, flops,
+                   (split ? 4.0 : 2.0) * ((double)M * K + (double)N * K) + 8.0 * M * N, M, N, K);
+    if (split)
+        tc_gemm_sub_kernel<true><<<(unsigned)grid, 128, TcCfg<true>::kSmem, ctx->stream>>>(
+            ma, mb, mal, mbl, args);
+    else
+        tc_gemm_sub_kernel<false><<<(unsigned)grid, 128, TcCfg<false>::kSmem, ctx->stream>>>(
+            ma, mb, mal, mbl, args);
     ctx->launches++;
     return last_cuda(ctx);
+}
+}  // namespace
+
+hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
+                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only)
+{
+    return tc_launch(ctx, fmt, M, N, K, A, B, nullptr, nullptr, C, ldc, scale, lower_only);
+}
+
+hdbf_status tc_gemm_sub_split(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
+                              const TcOperand& Alo, const TcOperand& B, const TcOperand& Blo,
+                              float* C, long long ldc, float scale, bool lower_only)
+{
+    return tc_launch(ctx, fmt, M, N, K, A, B, &Alo, &Blo, C, ldc, scale, lower_only);
 }
 
 }  // namespace hdbf
