@@ -354,19 +354,44 @@ apply_moves_smem_kernel(float* A, long long lda, int ncols, const int* __restric
                         const int* __restrict__ tgt, const int* __restrict__ count, int cpc,
                         int cap)
 {
-    extern __shared__ float buf[];
+    extern __shared__ float buf[];  // cpc * cap values, then cap sources, cap targets
+    int* s_src = reinterpret_cast<int*>(buf + (size_t)cpc * cap);
+    int* s_tgt = s_src + cap;
     const int cnt = min(*count, cap);
     if (cnt <= 0) return;
     const int c0 = blockIdx.x * cpc;
     const int nc = min(cpc, ncols - c0);
-    for (int cc = 0; cc < nc; ++cc) {
-        const float* col = A + (long long)(c0 + cc) * lda;
-        for (int i = threadIdx.x; i < cnt; i += kApplyThreads) buf[cc * cap + i] = col[src[i]];
+    for (int i = threadIdx.x; i < cnt; i += kApplyThreads) {
+        s_src[i] = src[i];
+        s_tgt[i] = tgt[i];
     }
     __syncthreads();
-    for (int cc = 0; cc < nc; ++cc) {
-        float* col = A + (long long)(c0 + cc) * lda;
-        for (int i = threadIdx.x; i < cnt; i += kApplyThreads) col[tgt[i]] = buf[cc * cap + i];
+    // Flattened (column, move) space, eight independent loads in flight.
+    const int total = nc * cnt;
+    const float* base = A + (long long)c0 * lda;
+    int e = threadIdx.x;
+    for (; e + 7 * kApplyThreads < total; e += 8 * kApplyThreads) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = e + u * kApplyThreads, cc = q / cnt, i = q - cc * cnt;
+            v[u] = base[(long long)cc * lda + s_src[i]];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = e + u * kApplyThreads, cc = q / cnt, i = q - cc * cnt;
+            buf[cc * cap + i] = v[u];
+        }
+    }
+    for (; e < total; e += kApplyThreads) {
+        const int cc = e / cnt, i = e - cc * cnt;
+        buf[cc * cap + i] = base[(long long)cc * lda + s_src[i]];
+    }
+    __syncthreads();
+    float* wbase = A + (long long)c0 * lda;
+    for (int q = threadIdx.x; q < total; q += kApplyThreads) {
+        const int cc = q / cnt, i = q - cc * cnt;
+        wbase[(long long)cc * lda + s_tgt[i]] = buf[cc * cap + i];
     }
 }
 
@@ -483,15 +508,16 @@ hdbf_status apply_moves(hdbf_context* ctx, float* A, long long lda, int ncols,
 {
     if (ncols <= 0 || max_moves <= 0) return HDBF_STATUS_SUCCESS;
     const size_t per_col = (size_t)max_moves * sizeof(float);
-    const size_t budget = 48 * 1024;
+    const size_t idx_bytes = 2 * (size_t)max_moves * sizeof(int);
+    const size_t budget = 64 * 1024;
     const size_t hard_cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
     ProfScope prof(ctx, kClsMoves, 0.0, 8.0 * (double)max_moves * ncols);
-    if (per_col <= hard_cap) {
-        int cpc = (int)(budget / per_col);
+    if (per_col + idx_bytes <= hard_cap) {
+        int cpc = (int)((budget > idx_bytes ? budget - idx_bytes : 0) / per_col);
         if (cpc < 1) cpc = 1;
         if (cpc > 16) cpc = 16;
         const int grid = (ncols + cpc - 1) / cpc;
-        apply_moves_smem_kernel<<<grid, kApplyThreads, per_col * cpc, ctx->stream>>>(
+        apply_moves_smem_kernel<<<grid, kApplyThreads, per_col * cpc + idx_bytes, ctx->stream>>>(
             A, lda, ncols, src, tgt, count, cpc, max_moves);
         ctx->launches++;
         return last_cuda(ctx);
