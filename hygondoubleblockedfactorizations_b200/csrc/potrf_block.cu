@@ -4,20 +4,23 @@
 // Replaces the reference's rocsolver_spotrf call on the diagonal block
 // (src/potrf/double_blocked_potrf.cpp:34-56, call :334).  The block is cut
 // into 64 x 64 tiles (NT = ceil(n / 64) <= 16) and factored right-looking:
-// for every tile column k one CTA factors the diagonal tile (register-resident
-// potf2) and inverts it, then CTAs solve the tiles below it against that
-// inverse, then CTAs apply the rank-64 update to the trailing tiles -- three
-// phases separated by bounded grid barriers.  With the inverse requested,
-// W = L^{-1} (lower, the strictly upper tiles zeroed) is formed tile diagonal
-// by tile diagonal: W(i,j) = -D_i sum_{m=j}^{i-1} L(i,m) W(m,j), D_i = L(i,i)^{-1}.
-// A recursive factorization of the same block issues ~100 small launches;
-// here the latency chain is 3 NT barriers plus NT tile factorizations.
+// for every tile column k the CTAs solve the tiles below the diagonal against
+// the inverse D_k of the factored diagonal tile, then apply the rank-64 update
+// to the trailing tiles; with look-ahead, CTA 0 updates tile (k+1, k+1) first
+// and factors and inverts it (register-resident potf2) while the other CTAs
+// finish the update -- two bounded grid barriers per tile column.  With the
+// inverse requested, W = L^{-1} (lower, the strictly upper tiles zeroed) is
+// formed by recursive doubling over tile blocks: for siblings A and C,
+// W(C,A) = -W(C,C) (L(C,A) W(A,A)), two GEMM phases per level.
+// A recursive factorization of the same block issues ~100 small launches.
 //
 // Pivot test and info follow LAPACK xPOTRF: the first column whose updated
 // diagonal is not > 0 (or is NaN) stops the factorization and info =
 // info_base + column + 1 (first failure wins); a block whose info is already
 // non-zero is left untouched.  Every grid-barrier wait is bounded: on expiry
 // the kernel records a timeout, and later barriers return at once.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace hdbf {
@@ -192,7 +195,8 @@ __device__ void tri_inv_tile(const float* L, long long ld, int nb, float* Ls /*6
 
 __global__ void __launch_bounds__(kThreads, 1)
 potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, float* W,
-                   long long ldw, float* dinv, unsigned* ctr, int* fail, int* abort_flag, int* err)
+                   long long ldw, float* dinv, float* Tsc, unsigned* ctr, int* fail,
+                   int* abort_flag, int* err)
 {
     __shared__ __align__(16) float As[kT * kLdS];
     __shared__ __align__(16) float Bs[kT * kLdS];
@@ -213,27 +217,54 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
     grid_barrier(sy);
     if (skip) return;
 
-    bool ok = true;
-    for (int k = 0; k < NT && ok; ++k) {
-        // P1: factor and invert the diagonal tile
-        if (cta == 0) {
-            const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d);
-            if (f >= 0) {
-                if (tid == 0) {
-                    if (info) atomicCAS(info, 0, info_base + k * kT + f + 1);
-                    atomicExch(fail, 1);
-                }
-            } else {
-                __syncthreads();
-                tri_inv_tile(tile(k, k), lda, ext(k), As, dinv + (long long)k * kT * kT);
+    // Factor (and invert) diagonal tile k on this CTA; false on a bad pivot.
+    auto factor_diag = [&](int k) -> bool {
+        const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d);
+        if (f >= 0) {
+            if (tid == 0) {
+                if (info) atomicCAS(info, 0, info_base + k * kT + f + 1);
+                atomicExch(fail, 1);
             }
+            return false;
         }
-        grid_barrier(sy);
+        __syncthreads();
+        tri_inv_tile(tile(k, k), lda, ext(k), As, dinv + (long long)k * kT * kT);
+        return true;
+    };
+    // A(i,j) -= L(i,k) L(j,k)^T (lower part only on the diagonal)
+    auto update_tile = [&](int k, int i, int j) {
+        load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
+        load_kmajor(Bs, tile(j, k), lda, ext(j), ext(k));
+        __syncthreads();
+        float acc[4][4] = {};
+        tile_mma(acc, As, Bs);
+        float* T = tile(i, j);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = ty * 4 + a, c = tx * 4 + b;
+                if (r < ext(i) && c < ext(j) && (i != j || r >= c)) {
+                    const long long o = (long long)c * lda + r;
+                    T[o] = __ldcg(T + o) - acc[a][b];
+                }
+            }
+        __syncthreads();
+    };
+    auto failed = [&]() -> bool {
         if (tid == 0) s_flag = *reinterpret_cast<volatile int*>(fail) |
                                *reinterpret_cast<volatile int*>(abort_flag);
         __syncthreads();
-        if (s_flag) { ok = false; break; }
-        if (k == NT - 1) break;
+        return s_flag != 0;
+    };
+
+    // Right-looking over tile columns with look-ahead: during the trailing
+    // update of step k, CTA 0 first updates tile (k+1, k+1) and factors it
+    // while the other CTAs update the remaining tiles.
+    if (cta == 0) factor_diag(0);
+    grid_barrier(sy);
+    bool ok = !failed();
+    for (int k = 0; k < NT - 1 && ok; ++k) {
         // P2: L(i,k) = A(i,k) D_k^T for i > k
         for (int i = k + 1 + cta; i < NT; i += G) {
             load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
@@ -252,36 +283,32 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
             __syncthreads();
         }
         grid_barrier(sy);
-        // P3: A(i,j) -= L(i,k) L(j,k)^T for k < j <= i
+        // P3 (+ P1 of step k+1 on CTA 0): pairs t >= 1 on CTAs 1.., t = 0 is
+        // tile (k+1, k+1)
         const int rem = NT - 1 - k;
         const int pairs = rem * (rem + 1) / 2;
-        for (int t = cta; t < pairs; t += G) {
-            int i = k + 1, j = k + 1, left = t;
-            while (left > i - (k + 1)) { left -= i - k; ++i; }
-            j = k + 1 + left;
-            load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
-            load_kmajor(Bs, tile(j, k), lda, ext(j), ext(k));
-            __syncthreads();
-            float acc[4][4] = {};
-            tile_mma(acc, As, Bs);
-            float* T = tile(i, j);
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const int r = ty * 4 + a, c = tx * 4 + b;
-                    if (r < ext(i) && c < ext(j) && (i != j || r >= c)) {
-                        const long long o = (long long)c * lda + r;
-                        T[o] = __ldcg(T + o) - acc[a][b];
-                    }
-                }
-            __syncthreads();
+        if (cta == 0) {
+            update_tile(k, k + 1, k + 1);
+            factor_diag(k + 1);
+        }
+        const int workers = G > 1 ? (int)G - 1 : 1;
+        const int first = G > 1 ? cta - 1 : 0;
+        if (G == 1 || cta > 0) {
+            for (int t = 1 + first; t < pairs; t += workers) {
+                int i = k + 1, left = t;
+                while (left > i - (k + 1)) { left -= i - k; ++i; }
+                update_tile(k, i, k + 1 + left);
+            }
         }
         grid_barrier(sy);
+        if (failed()) { ok = false; break; }
     }
     if (!ok || !W) return;
 
-    // W = L^{-1}: diagonal tiles D_i, strictly upper tiles zero
+    // W = L^{-1} by recursive doubling over tile blocks: for sibling blocks
+    // A = [b, b+s) and C = [b+s, b+2s) (tiles), W(C,A) = -W(C,C) (L(C,A) W(A,A)),
+    // T = L(C,A) W(A,A) kept in scratch at the W(C,A) position.
+    // Setup: diagonal tiles D_i, strictly upper tiles zero.
     for (int t = cta; t < NT * NT; t += G) {
         const int i = t % NT, j = t / NT;
         if (i < j) {
@@ -299,35 +326,58 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
         }
     }
     grid_barrier(sy);
-    for (int d = 1; d < NT; ++d) {
-        for (int i = d + cta; i < NT; i += G) {
-            const int j = i - d;
+    auto wt = [&](int i, int j) { return W + (long long)(j * kT) * ldw + i * kT; };
+    auto tt = [&](int i, int j) { return Tsc + (long long)(j * kT) * ldw + i * kT; };
+    for (int st = 1; st < NT; st *= 2) {
+        // tiles (ci, aj) of every pair: C rows [b+st, min(b+2st, NT)), A cols [b, b+st)
+        const int npair = (NT + 2 * st - 1) / (2 * st);
+        const int per = st * st;
+        // phase A: T(ci, aj) = sum_{m=aj}^{b+st-1} L(ci, m) W(m, aj)
+        for (int t = cta; t < npair * per; t += G) {
+            const int pr = t / per, q = t - pr * per;
+            const int b = pr * 2 * st;
+            const int ci = b + st + q / st, aj = b + q % st;
+            if (ci >= NT) continue;
             float acc[4][4] = {};
-            for (int m = j; m < i; ++m) {
-                load_kmajor(As, tile(i, m), lda, ext(i), ext(m));
-                load_trans(Bs, W + (long long)(j * kT) * ldw + m * kT, ldw, ext(m), ext(j));
+            for (int m = aj; m < b + st; ++m) {
+                load_kmajor(As, tile(ci, m), lda, ext(ci), ext(m));
+                load_trans(Bs, wt(m, aj), ldw, ext(m), ext(aj));
                 __syncthreads();
                 tile_mma(acc, As, Bs);
                 __syncthreads();
             }
-            // W(i,j) = -D_i acc
-            load_kmajor(As, dinv + (long long)i * kT * kT, kT, ext(i), ext(i));
+            float* T = tt(ci, aj);
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) Bs[(ty * 4 + a) * kLdS + tx * 4 + b] = acc[a][b];
-            __syncthreads();
-            float w[4][4] = {};
-            tile_mma(w, As, Bs);
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const int r = ty * 4 + a, c = tx * 4 + b;
-                    if (r < ext(i) && c < ext(j))
-                        W[(long long)(j * kT + c) * ldw + i * kT + r] = -w[a][b];
+                for (int bb = 0; bb < 4; ++bb) {
+                    const int r = ty * 4 + a, c = tx * 4 + bb;
+                    if (r < ext(ci) && c < ext(aj)) T[(long long)c * ldw + r] = acc[a][bb];
                 }
-            __syncthreads();
+        }
+        grid_barrier(sy);
+        // phase B: W(ci, aj) = -sum_{m=b+st}^{ci} W(ci, m) T(m, aj)
+        for (int t = cta; t < npair * per; t += G) {
+            const int pr = t / per, q = t - pr * per;
+            const int b = pr * 2 * st;
+            const int ci = b + st + q / st, aj = b + q % st;
+            if (ci >= NT) continue;
+            float acc[4][4] = {};
+            for (int m = b + st; m <= ci; ++m) {
+                load_kmajor(As, wt(ci, m), ldw, ext(ci), ext(m));
+                load_trans(Bs, tt(m, aj), ldw, ext(m), ext(aj));
+                __syncthreads();
+                tile_mma(acc, As, Bs);
+                __syncthreads();
+            }
+            float* Wp = wt(ci, aj);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    const int r = ty * 4 + a, c = tx * 4 + bb;
+                    if (r < ext(ci) && c < ext(aj)) Wp[(long long)c * ldw + r] = -acc[a][bb];
+                }
         }
         grid_barrier(sy);
     }
@@ -342,7 +392,9 @@ hdbf_status potrf_block(hdbf_context* ctx, int n, float* A, long long lda, int* 
 {
     if (n <= 0) return HDBF_STATUS_SUCCESS;
     if (n > kT * kMaxNT || lda < n || (W && ldw < n)) return HDBF_STATUS_INVALID_VALUE;
-    HDBF_TRY(ensure_ws(ctx, n));
+    // ws_skinny holds 256 * ws_n floats: >= n * ldw once ws_n >= max(n, ldw * n / 256)
+    const long long need = W ? ((long long)ldw * n + 255) / 256 : 0;
+    HDBF_TRY(ensure_ws(ctx, (int)std::max<long long>(n, std::max<long long>(need, 64))));
     const int NT = (n + kT - 1) / kT;
     int G = NT * (NT - 1) / 2;
     if (W && NT * NT > G) G = NT * NT;  // the W set-up pass touches NT^2 tiles
@@ -355,10 +407,11 @@ hdbf_status potrf_block(hdbf_context* ctx, int n, float* A, long long lda, int* 
     int* abort_flag = sm + 2;
     int* err = ctx->dev_small + kSmallErr;
     float* dinv = ws_inv(ctx);
+    float* Tsc = ws_skinny(ctx);  // n x n scratch (leading dimension ldw) for the inverse
     const double flops = (double)n * n * n / 3.0 + (W ? (double)n * n * n / 3.0 : 0.0);
     ProfScope prof(ctx, kClsPotrfBlock, flops, 8.0 * n * n, n, n, n);
-    void* args[] = {&n, &A, &lda, &info, &info_base, &W, &ldw, &dinv, &ctr, &fail, &abort_flag,
-                    &err};
+    void* args[] = {&n, &A, &lda, &info, &info_base, &W, &ldw, &dinv, &Tsc, &ctr, &fail,
+                    &abort_flag, &err};
     const cudaError_t e = cudaLaunchCooperativeKernel((const void*)potrf_block_kernel, dim3(G),
                                                       dim3(kThreads), args, 0, ctx->stream);
     ctx->launches++;
