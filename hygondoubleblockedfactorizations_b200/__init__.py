@@ -44,6 +44,7 @@ _PROTOS = {
     "hdbf_profile_num_classes": (c_int, []),
     "hdbf_set_graph_mode": (c_int, [P, c_int]),
     "hdbf_set_panel_kernel": (c_int, [P, c_int]),
+    "hdbf_set_lookahead": (c_int, [P, c_int]),
     # potrf
     "double_blocked_potrf": (None, [P, P, c_int, c_int, c_int, c_int, P]),
     "double_blocked_potrf_dbtrsm": (None, [P, P, c_int, c_int, c_int, c_int, P]),
@@ -195,6 +196,12 @@ class Handle:
         st = lib().hdbf_set_panel_kernel(self._h, int(mode))
         if st != 0:
             raise HdbfError(f"set_panel_kernel: {status_string(st)}")
+
+    def set_lookahead(self, enabled: bool):
+        """Overlap the GETRF panel chain with the outer update (batched/no pivoting)."""
+        st = lib().hdbf_set_lookahead(self._h, 1 if enabled else 0)
+        if st != 0:
+            raise HdbfError(f"set_lookahead: {status_string(st)}")
 
     def set_graphs(self, enabled: bool):
         lib().hdbf_set_graph_mode(self._h, 1 if enabled else 0)

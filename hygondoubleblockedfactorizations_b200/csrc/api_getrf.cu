@@ -83,9 +83,37 @@ hdbf_status gemm_nn_rows(hdbf_context* ctx, int rows, int cols, int k, const flo
 
 enum class PivotMode { Immediate, Batched, None };
 
+// Launchers enqueue on ctx->stream; the look-ahead panel chain points it at
+// the internal stream for the duration of a scope.
+struct OnStream {
+    hdbf_context* ctx;
+    cudaStream_t saved;
+    OnStream(hdbf_context* c, cudaStream_t s) : ctx(c), saved(c->stream) { c->stream = s; }
+    ~OnStream() { ctx->stream = saved; }
+};
+
+struct NoSkinny {
+    hdbf_context* ctx;
+    explicit NoSkinny(hdbf_context* c) : ctx(c) { c->no_skinny = true; }
+    ~NoSkinny() { ctx->no_skinny = false; }
+};
+
 // Double-blocked left-looking LU (src/getrf/double_blocked_getrf.cpp:125-191,
 // src/getrf/getrf_batched_pivot_internal.h:445-624,
 // src/getrf/double_blocked_getrf_npvt.cpp:93-144).
+//
+// Look-ahead (batched or no pivoting, hdbf_set_lookahead): the outer TRSM of
+// block b+1 runs whole, then its outer GEMM (K = all previous columns) is
+// enqueued on the caller's stream in column chunks of whole inner panels,
+// each followed by an event; the inner-panel chain of block b+1 (panel, row
+// interchanges, inner TRSM + GEMM) runs on the high-priority internal stream
+// and waits only for the chunk it is about to touch, so panel factorizations
+// overlap the rest of the outer GEMM.  The chain joins the caller's stream
+// before the block's outer pivot batch.  Interchanges of a block's panels
+// reach each later inner panel of the block as one composed permutation just
+// before its inner update (instead of one permutation per panel), because
+// the outer GEMM may still be writing those columns; the composition is kept
+// running across the block's panels, and the data movement is the same.
 hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer_nb,
                           int inner_nb, bool iterative_outer, int trsm_block,
                           int inner_gemm_m_tile, int* ipiv, int* info, PivotMode mode,
@@ -109,14 +137,36 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
     if (inner_nb <= 0) inner_nb = outer_nb;
     inner_nb = std::min(inner_nb, outer_nb);
     const bool piv = mode != PivotMode::None;
+    bool la = ctx->lookahead && mode != PivotMode::Immediate && n > outer_nb &&
+              n + inner_nb <= compose_running_max_m(ctx);
+    if (la && !ctx->la_stream) {
+        // The stream and events are created outside any capture.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess ||
+            cs != cudaStreamCaptureStatusNone || ensure_lookahead(ctx) != HDBF_STATUS_SUCCESS) {
+            cudaGetLastError();
+            la = false;
+        }
+    }
     const std::vector<long long> key = {
         10 + (int)mode, (long long)A, lda, n, outer_nb, inner_nb, iterative_outer, trsm_block,
         inner_gemm_m_tile, (long long)ipiv, (long long)info, (long long)ws.src, (long long)ws.tgt,
-        (long long)ws.temp, ws.temp_cols};
+        (long long)ws.temp, ws.temp_cols, la ? 1 : 0};
     return run_graph(ctx, key, [&]() -> hdbf_status {
     if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
-    for (int outer = 0; outer < n; outer += outer_nb) {
-        const int oend = outer + std::min(outer_nb, n - outer);
+    const cudaStream_t main_s = ctx->stream;
+    int nchunks = 0;  // outer-update chunks of the current block (look-ahead)
+    int chunk_w = 0;  // their width in columns (whole inner panels)
+
+    // Inner panels of one outer block [outer, oend).
+    auto block_chain = [&](int outer, int oend, bool forked) -> hdbf_status {
+        int waited = 0;
+        auto wait_chunk = [&](int col) {
+            const int c = (col - outer) / chunk_w;
+            while (waited <= c && waited < nchunks)
+                cudaStreamWaitEvent(ctx->stream, ctx->la_ev[waited++], 0);
+        };
+        if (forked) wait_chunk(outer);
         for (int inner = outer; inner < oend; inner += inner_nb) {
             const int isz = std::min(inner_nb, oend - inner);
             const int next = inner + isz;
@@ -129,13 +179,22 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
                                       cb, cc, 2));
             } else if (mode == PivotMode::Batched) {
                 const int cb[2] = {outer, next};
-                const int cc[2] = {inner - outer, oend - next};
+                const int cc[2] = {inner - outer, la ? 0 : oend - next};
                 HDBF_TRY(permute_cols(ctx, ws, A, lda, n, inner, ipiv + inner, isz, inner, info,
                                       cb, cc, 2));
             }
             if (next < oend) {  // prepare_next_inner_panel
                 const int nsz = std::min(inner_nb, oend - next);
                 const int hist = next - outer;
+                if (forked) wait_chunk(next);
+                if (la && mode == PivotMode::Batched) {  // the block's interchanges so far
+                    HDBF_TRY(compose_running(ctx, ipiv + outer, inner - outer, hist, outer,
+                                             n - outer, ws_perm(ctx), inner == outer, ws.src,
+                                             ws.tgt, ws.count, info));
+                    HDBF_TRY(apply_moves(ctx, at(A, lda, outer, next), lda, nsz, ws.src, ws.tgt,
+                                         ws.count, std::min(n - outer, 2 * hist), ws.temp,
+                                         ws.temp_cols));
+                }
                 HDBF_TRY(trsm_llu(ctx, hist, nsz, at(A, lda, outer, outer), lda,
                                   at(A, lda, outer, next), lda));
                 HDBF_TRY(gemm_nn_rows(ctx, n - next, nsz, hist, at(A, lda, next, outer), lda,
@@ -143,6 +202,25 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
                                       mode == PivotMode::Batched ? inner_gemm_m_tile : 0));
             }
         }
+        return HDBF_STATUS_SUCCESS;
+    };
+
+    for (int outer = 0; outer < n; outer += outer_nb) {
+        const int oend = outer + std::min(outer_nb, n - outer);
+        if (nchunks > 0) {
+            ctx->la_used = true;
+            hdbf_status st;
+            {
+                OnStream on(ctx, ctx->la_stream);
+                st = block_chain(outer, oend, true);
+                cudaEventRecord(ctx->la_ev[kLaEvents - 1], ctx->la_stream);
+            }
+            cudaStreamWaitEvent(main_s, ctx->la_ev[kLaEvents - 1], 0);
+            HDBF_TRY(st);
+        } else {
+            HDBF_TRY(block_chain(outer, oend, false));
+        }
+        nchunks = 0;
         if (mode == PivotMode::Batched) {  // outer pivot batch (:556-609)
             if (outer > 0) {
                 const int cb[1] = {0};
@@ -161,8 +239,22 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
             const int nsz = std::min(outer_nb, n - next);
             HDBF_TRY(trsm_llu_mode(ctx, next, nsz, A, lda, at(A, lda, 0, next), lda,
                                    iterative_outer, trsm_block));
-            HDBF_TRY(sgemm_sub(ctx, true, false, n - next, nsz, next, at(A, lda, next, 0), lda,
-                               at(A, lda, 0, next), lda, at(A, lda, next, next), lda));
+            if (la) {
+                const int panels = (nsz + inner_nb - 1) / inner_nb;
+                const int group = (panels + kLaEvents - 2) / (kLaEvents - 1);
+                chunk_w = group * inner_nb;
+                NoSkinny ns(ctx);  // the panel chain may use the split-K scratch
+                for (int c0 = 0; c0 < nsz; c0 += chunk_w) {
+                    const int cw = std::min(chunk_w, nsz - c0);
+                    HDBF_TRY(sgemm_sub(ctx, true, false, n - next, cw, next, at(A, lda, next, 0),
+                                       lda, at(A, lda, 0, next + c0), lda,
+                                       at(A, lda, next, next + c0), lda));
+                    cudaEventRecord(ctx->la_ev[nchunks++], main_s);
+                }
+            } else {
+                HDBF_TRY(sgemm_sub(ctx, true, false, n - next, nsz, next, at(A, lda, next, 0), lda,
+                                   at(A, lda, 0, next), lda, at(A, lda, next, next), lda));
+            }
         }
     }
     return last_cuda(ctx);

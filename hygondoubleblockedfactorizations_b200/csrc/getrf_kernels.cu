@@ -7,9 +7,11 @@
 // the CTAs publish their local |max| candidate (value, row and the full
 // candidate row) and the owner of the diagonal row publishes that row, then
 // exchange them through global memory (see the protocol note below), after
-// which every CTA picks the same global winner (largest |a|, lowest row on ties -- LAPACK ISAMAX), swaps,
-// scales by the reciprocal pivot (division when |pivot| < FLT_MIN, as
-// xGETF2) and applies the rank-1 update to its own rows.
+// which every CTA picks the same global winner (largest |a|, lowest row on
+// ties -- LAPACK ISAMAX), swaps, scales by the reciprocal pivot (division
+// when |pivot| < FLT_MIN, as xGETF2) and applies the rank-1 update to its own
+// rows -- the next column first, so that its candidate is published before
+// the rest of the update runs.
 //
 // compose_swaps + apply_moves replace apply_panel_pivots_kernel
 // (src/getrf/getrf_pivot_kernels.hip:14-45) and the host-side permutation
@@ -28,19 +30,20 @@ namespace {
 constexpr int kCoopThreads = 256;
 constexpr int kCoopMaxW = 128;
 constexpr int kCoopMaxGrid = 256;
-// Per-(parity, CTA) exchange slot: [seq, |val|, row, pad | cand row (32) | diag row (32)]
-constexpr int kSlotFloats = 4 + 2 * kCoopMaxW;
+// Per-(parity, CTA) exchange slot, in 64-bit words:
+// [header, pad | candidate row (kCoopMaxW) | diagonal row (kCoopMaxW)]
+constexpr int kSlotWords = 2 + 2 * kCoopMaxW;
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
 {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
 {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // Candidate (v, i) beats (bv, bi): a real row beats none, then larger |a|,
@@ -81,29 +84,43 @@ __device__ __forceinline__ void coop_move(float* A, long long lda, float* tile, 
     }
 }
 
-// Exchange protocol (no grid barrier): for column j every CTA writes its slot
-// (parity j&1) -- candidate |max|, its row index and that row's w values, plus
-// the diagonal row j if it owns it -- then publishes seq = epoch*64 + j + 1
-// with a release store.  Every CTA polls all G seq words with acquire loads
-// (bounded), reduces the candidates identically, and fetches the winning row
-// and the old diagonal row.  A CTA can only overwrite a parity slot after all
-// CTAs have published the following column, i.e. after every CTA finished
-// reading that slot, so two parities suffice.  `epoch` is read at entry and
-// advanced by the last CTA to finish, so slots of earlier launches (and of
-// earlier CUDA-graph replays) never match.
+constexpr unsigned kNoRow = 0xffffu;  // "no candidate" in the header
+
+// Exchange protocol (no grid barrier, no fences).  Slot (parity, CTA) holds
+// 64-bit words, each written and read whole (single-copy atomic):
+//   header  [ |a| bits : 32 | column + 1 : 16 | local row : 16 ]
+//   rows    [ tag : 32 | value bits : 32 ] for the CTA's candidate row and,
+//           from the CTA owning it, the diagonal row; tag = epoch << 8 |
+//           column + 1, epoch = launch counter.
+// Column j uses parity j & 1.  Every CTA polls all G headers (thread q
+// watches CTA q, bounded) and then reads the winner's and the diagonal rows,
+// re-reading any word whose tag is not yet this column's: each word proves
+// its own freshness, so a writer needs no release fence between its rows and
+// its header, and one L2 trip delivers the flag with the candidate.  A CTA
+// only rewrites a parity after every CTA has published the following column,
+// i.e. after all of them finished reading it, so two parities suffice.  The
+// last CTA to finish zeroes every header (column 0 never matches) and
+// advances the epoch, so no launch accepts an earlier launch's words.
+//
+// Look-ahead inside the column loop: after the pivot of column j is applied,
+// each CTA updates only column j + 1 of its rows, publishes its column-(j+1)
+// candidate and then runs the rest of the rank-1 update while the exchange
+// is in flight.  The published rows therefore still lack step j's update in
+// columns > j + 1; the receivers finish them with the row's own multiplier
+// (its column-j entry) and the step-j pivot row -- the same fmaf the owner
+// applies to its copy, so every CTA holds bit-identical rows.
 __global__ void __launch_bounds__(kCoopThreads)
 getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int ipiv_add,
-                  int* info, int info_base, float* scr, unsigned* epoch_ptr, unsigned* done_ptr,
-                  int* err, int pivot)
+                  int* info, int info_base, unsigned long long* scr, unsigned* epoch_ptr,
+                  unsigned* done_ptr, int* err, int pivot)
 {
     extern __shared__ float tile[];  // tile[c * rpc + r]
-    __shared__ float prow[kCoopMaxW];
-    __shared__ float orow[kCoopMaxW];
+    __shared__ float prow_s[2][kCoopMaxW];  // pivot rows of the last two columns
     __shared__ float red_v[kCoopThreads / 32];
     __shared__ int red_i[kCoopThreads / 32];
     __shared__ float cv[kCoopMaxGrid];
     __shared__ int ci[kCoopMaxGrid];
-    __shared__ int s_best_row, s_win_cta, s_abort;
+    __shared__ int s_abort, s_last;
 
     const int G = gridDim.x;
     const int cta = blockIdx.x;
@@ -111,67 +128,82 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     const int lane = tid & 31, warp = tid >> 5;
     const int r0 = cta * rpc;
     const int nr = max(0, min(m, r0 + rpc) - r0);
+    const int steps = min(m, w);
     const unsigned epoch = *reinterpret_cast<volatile unsigned*>(epoch_ptr);
+    auto slot_of = [&](int par, int q) {
+        return scr + ((long long)par * kCoopMaxGrid + q) * kSlotWords;
+    };
+    auto row_tag = [&](int col) { return (epoch << 8) | (unsigned)(col + 1); };
 
     coop_move<true>(A + r0, lda, tile, rpc, nr, w);
     if (tid == 0) s_abort = 0;
     __syncthreads();
 
-    const int steps = min(m, w);
-    for (int j = 0; j < steps; ++j) {
-        const int par = j & 1;
-        const unsigned seq = (epoch << 6) + (unsigned)j + 1u;
-        float* slot = scr + ((long long)par * kCoopMaxGrid + cta) * kSlotFloats;
-        const int owner = j / rpc;
-
-        // 1. local candidate over owned rows >= j (largest |a|, lowest row)
+    // Block-wide candidate of column `col` over owned rows >= col, from the
+    // values now in the tile; every thread returns the same local row (or -1).
+    auto block_candidate = [&](int col, float& val) -> int {
         float bv = -1.f;
         int bi = INT_MAX;
-        if (pivot) {
-            for (int r = tid; r < nr; r += kCoopThreads) {
-                const int gr = r0 + r;
-                if (gr >= j) {
-                    const float v = fabsf(tile[j * rpc + r]);
-                    if (bi == INT_MAX || v > bv) { bv = v; bi = gr; }
-                }
+        for (int r = tid; r < nr; r += kCoopThreads) {
+            if (r0 + r >= col) {
+                const float v = fabsf(tile[col * rpc + r]);
+                if (bi == INT_MAX || v > bv) { bv = v; bi = r0 + r; }
             }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const float ov = __shfl_down_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-                if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
-            }
-            if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
-            __syncthreads();
-            if (tid == 0) {
-                for (int q = 1; q < kCoopThreads / 32; ++q)
-                    if (better(red_v[q], red_i[q], bv, bi)) { bv = red_v[q]; bi = red_i[q]; }
-                s_best_row = bi;
-                red_v[0] = bv;
-            }
-            __syncthreads();
         }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ov = __shfl_down_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+        __syncthreads();
+        bv = red_v[0];
+        bi = red_i[0];
+#pragma unroll
+        for (int q = 1; q < kCoopThreads / 32; ++q)
+            if (better(red_v[q], red_i[q], bv, bi)) { bv = red_v[q]; bi = red_i[q]; }
+        val = bv;
+        return bi == INT_MAX ? -1 : bi - r0;
+    };
 
-        // 2. publish
-        const int my_best = pivot ? s_best_row : INT_MAX;
+    // Publish column `col`: candidate row (local index lr, or -1), the
+    // diagonal row if owned, and the header (no ordering needed among them).
+    auto publish = [&](int col, int lr, float val) {
+        unsigned long long* slot = slot_of(col & 1, cta);
+        const unsigned long long t = (unsigned long long)row_tag(col) << 32;
+        const bool own_diag = col >= r0 && col < r0 + nr;
         if (tid < w) {
-            if (my_best != INT_MAX) slot[4 + tid] = tile[tid * rpc + (my_best - r0)];
-            if (cta == owner) slot[4 + kCoopMaxW + tid] = tile[tid * rpc + (j - r0)];
+            if (lr >= 0) st_relaxed_u64(slot + 2 + tid, t | __float_as_uint(tile[tid * rpc + lr]));
+            if (own_diag)
+                st_relaxed_u64(slot + 2 + kCoopMaxW + tid,
+                               t | __float_as_uint(tile[tid * rpc + (col - r0)]));
         }
         if (tid == 0) {
-            slot[1] = pivot ? red_v[0] : -1.f;
-            slot[2] = __int_as_float(my_best);
+            const unsigned lo = ((unsigned)(col + 1) << 16) | (lr >= 0 ? (unsigned)lr : kNoRow);
+            const unsigned hi = lr >= 0 ? __float_as_uint(val) : __float_as_uint(-1.f);
+            st_relaxed_u64(slot, ((unsigned long long)hi << 32) | lo);
         }
-        __syncthreads();
-        // The release store (after the barrier) orders every thread's slot
-        // writes before the sequence number that other CTAs acquire.
-        if (tid == 0) st_release_u32(reinterpret_cast<unsigned*>(slot), seq);
+        __syncthreads();  // the rows were read before the rank-1 update rewrites them
+    };
 
-        // 3. poll every slot (thread q watches CTA q), bounded
+    if (steps > 0) {  // column 0 candidates, nothing to finish on the receiving side
+        float v = -1.f;
+        int lr = -1;
+        if (pivot) lr = block_candidate(0, v);
+        publish(0, lr, v);
+    }
+
+    for (int j = 0; j < steps; ++j) {
+        const int par = j & 1;
+        const unsigned tag = (unsigned)j + 1u;
+
+        // 1. every candidate header of column j (thread q watches CTA q), bounded
         for (int q = tid; q < G; q += kCoopThreads) {
-            const float* sq = scr + ((long long)par * kCoopMaxGrid + q) * kSlotFloats;
+            const unsigned long long* wq = slot_of(par, q);
             unsigned polls = 0;
-            while (ld_acquire_u32(reinterpret_cast<const unsigned*>(sq)) != seq) {
+            unsigned long long wv;
+            while (((unsigned)((wv = ld_relaxed_u64(wq)) >> 16) & 0xffffu) != tag) {
                 if (++polls > kSpinLimit) {
                     atomicExch(err, kErrTimeout);
                     s_abort = 1;
@@ -179,55 +211,83 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                 }
                 if (polls > 256) __nanosleep(32);
             }
-            cv[q] = __ldcg(sq + 1);
-            ci[q] = __float_as_int(__ldcg(sq + 2));
+            const unsigned lr = (unsigned)wv & 0xffffu;
+            cv[q] = __uint_as_float((unsigned)(wv >> 32));
+            ci[q] = lr == kNoRow ? INT_MAX : q * rpc + (int)lr;
         }
         __syncthreads();
         if (s_abort) break;
 
-        // 4. global winner, identical on every CTA
-        if (!pivot) {
-            if (tid == 0) { s_best_row = j; s_win_cta = -1; }
-        } else if (warp == 0) {
-            float gv = -1.f;
-            int gi = INT_MAX, gc = 0;
-            for (int q = lane; q < G; q += 32)
-                if (better(cv[q], ci[q], gv, gi)) { gv = cv[q]; gi = ci[q]; gc = q; }
+        // 2. the winner (each of the first warps reduces redundantly), its
+        // row and the diagonal row, finished with step j-1's update; swap.
+        const int owner = j / rpc;
+        float* prow = prow_s[par];
+        const float* prev = prow_s[par ^ 1];
+        if (tid < ((w + 31) & ~31)) {
+            int gi = j, gc = owner;
+            if (pivot) {
+                float gv = -1.f;
+                gi = INT_MAX;
+                for (int q = lane; q < G; q += 32)
+                    if (better(cv[q], ci[q], gv, gi)) { gv = cv[q]; gi = ci[q]; gc = q; }
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const float ov = __shfl_down_sync(0xffffffffu, gv, off);
-                const int oi = __shfl_down_sync(0xffffffffu, gi, off);
-                const int oc = __shfl_down_sync(0xffffffffu, gc, off);
-                if (better(ov, oi, gv, gi)) { gv = ov; gi = oi; gc = oc; }
+                for (int off = 16; off > 0; off >>= 1) {
+                    const float ov = __shfl_xor_sync(0xffffffffu, gv, off);
+                    const int oi = __shfl_xor_sync(0xffffffffu, gi, off);
+                    const int oc = __shfl_xor_sync(0xffffffffu, gc, off);
+                    if (better(ov, oi, gv, gi)) { gv = ov; gi = oi; gc = oc; }
+                }
+                if (gi == INT_MAX) { gi = j; gc = owner; }  // unreachable: row j always competes
             }
-            if (lane == 0) { s_best_row = gi; s_win_cta = gc; }
+            if (tid < w) {
+                // without pivoting the pivot row is the diagonal row
+                const unsigned long long* sw =
+                    pivot ? slot_of(par, gc) + 2 : slot_of(par, owner) + 2 + kCoopMaxW;
+                const unsigned long long* so = slot_of(par, owner) + 2 + kCoopMaxW;
+                const unsigned want = row_tag(j);
+                const bool fin = j > 0 && tid > j;
+                unsigned long long wp = ld_relaxed_u64(sw + tid), wo = ld_relaxed_u64(so + tid);
+                unsigned long long wl = fin ? ld_relaxed_u64(sw + (j - 1)) : 0ull;
+                unsigned long long wm = fin ? ld_relaxed_u64(so + (j - 1)) : 0ull;
+                unsigned polls = 0;
+                while ((unsigned)(wp >> 32) != want || (unsigned)(wo >> 32) != want ||
+                       (fin && ((unsigned)(wl >> 32) != want || (unsigned)(wm >> 32) != want))) {
+                    if (++polls > kSpinLimit) {
+                        atomicExch(err, kErrTimeout);
+                        s_abort = 1;
+                        break;
+                    }
+                    wp = ld_relaxed_u64(sw + tid);
+                    wo = ld_relaxed_u64(so + tid);
+                    if (fin) {
+                        wl = ld_relaxed_u64(sw + (j - 1));
+                        wm = ld_relaxed_u64(so + (j - 1));
+                    }
+                }
+                float pv = __uint_as_float((unsigned)wp), ov = __uint_as_float((unsigned)wo);
+                if (fin) {
+                    pv = fmaf(-__uint_as_float((unsigned)wl), prev[tid], pv);
+                    ov = fmaf(-__uint_as_float((unsigned)wm), prev[tid], ov);
+                }
+                prow[tid] = pv;
+                if (gi != j) {
+                    if (j >= r0 && j < r0 + nr) tile[tid * rpc + (j - r0)] = pv;
+                    if (gi >= r0 && gi < r0 + nr) tile[tid * rpc + (gi - r0)] = ov;
+                }
+            }
+            if (tid == 0 && pivot && cta == 0) ipiv[j] = gi + 1 + ipiv_add;
         }
         __syncthreads();
-        const int p = s_best_row;
-        if (tid < w) {
-            const float* so = scr + ((long long)par * kCoopMaxGrid + owner) * kSlotFloats;
-            orow[tid] = __ldcg(so + 4 + kCoopMaxW + tid);
-            if (s_win_cta >= 0) {
-                const float* sw = scr + ((long long)par * kCoopMaxGrid + s_win_cta) * kSlotFloats;
-                prow[tid] = __ldcg(sw + 4 + tid);
-            } else {
-                prow[tid] = orow[tid];
-            }
-        }
-        if (pivot && cta == 0 && tid == 0) ipiv[j] = p + 1 + ipiv_add;
-        __syncthreads();
+        if (s_abort) break;
 
-        // 5. swap rows j and p (within this column block), scale, rank-1 update
-        if (p != j && tid < w) {
-            if (j >= r0 && j < r0 + nr) tile[tid * rpc + (j - r0)] = prow[tid];
-            if (p >= r0 && p < r0 + nr) tile[tid * rpc + (p - r0)] = orow[tid];
-        }
-        __syncthreads();
+        // 3. scale column j, update column j+1 and find its candidate
         const float piv = prow[j];
         const bool nz = piv != 0.f;
         const bool recip = fabsf(piv) >= FLT_MIN;
         const float rcp = 1.0f / piv;
         if (!nz && cta == 0 && tid == 0 && info) atomicCAS(info, 0, info_base + j + 1);
+        const bool next = j + 1 < w;
+        const float pn = next ? prow[j + 1] : 0.f;
         for (int r = tid; r < nr; r += kCoopThreads) {
             if (r0 + r > j) {
                 float l = tile[j * rpc + r];
@@ -235,20 +295,51 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                     l = recip ? l * rcp : l / piv;
                     tile[j * rpc + r] = l;
                 }
-                for (int c = j + 1; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
+                if (next) tile[(j + 1) * rpc + r] = fmaf(-l, pn, tile[(j + 1) * rpc + r]);
             }
         }
-        __syncthreads();
+        if (j + 1 < steps) {
+            float v = -1.f;
+            int lr = -1;
+            if (pivot) lr = block_candidate(j + 1, v);  // its barrier orders the updates above
+            else __syncthreads();
+            publish(j + 1, lr, v);
+        }
+
+        // 4. the rest of step j's rank-1 update, overlapping the exchange
+        for (int r = tid; r < nr; r += kCoopThreads) {
+            if (r0 + r > j) {
+                const float l = tile[j * rpc + r];
+                int c = j + 2;
+                for (; c + 3 < w; c += 4) {
+                    const float t0 = tile[c * rpc + r], t1 = tile[(c + 1) * rpc + r];
+                    const float t2 = tile[(c + 2) * rpc + r], t3 = tile[(c + 3) * rpc + r];
+                    tile[c * rpc + r] = fmaf(-l, prow[c], t0);
+                    tile[(c + 1) * rpc + r] = fmaf(-l, prow[c + 1], t1);
+                    tile[(c + 2) * rpc + r] = fmaf(-l, prow[c + 2], t2);
+                    tile[(c + 3) * rpc + r] = fmaf(-l, prow[c + 3], t3);
+                }
+                for (; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
+            }
+        }
     }
+    __syncthreads();
 
     coop_move<false>(A + r0, lda, tile, rpc, nr, w);
 
-    // Advance the epoch once every CTA is done (the kernel's last action).
+    // The last CTA to finish clears every header of this launch and moves
+    // the epoch on.
     __syncthreads();
     if (tid == 0) {
         __threadfence();
-        const unsigned done = atomicAdd(done_ptr, 1u) + 1u;
-        if (done == (unsigned)G) {
+        s_last = atomicAdd(done_ptr, 1u) + 1u == (unsigned)G;
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int q = tid; q < 2 * G; q += kCoopThreads) *slot_of(q / G, q % G) = 0ull;
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
             atomicExch(done_ptr, 0u);
             atomicAdd(epoch_ptr, 1u);
         }
@@ -340,6 +431,80 @@ compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m,
         }
     }
     __syncthreads();
+    if (tid == 0) *count = s_base;
+}
+
+// Running composition for the GETRF look-ahead: the block's permutation is
+// kept in global memory between launches and staged in shared memory with the
+// new pivots; only the new swaps are replayed (one thread, inherently
+// ordered), then every displaced row becomes a move, in increasing target
+// order.
+__global__ void __launch_bounds__(kComposeThreads)
+compose_running_kernel(const int* __restrict__ ipiv, int k0, int k1, int ipiv_minus, int m,
+                       int* pos, int init, int* src, int* tgt, int* count, int* info, int* err)
+{
+    extern __shared__ int sp[];  // pos[m], then the pivots of [k0, k1)
+    __shared__ int warp_tot[kComposeThreads / 32];
+    __shared__ int s_base, s_bad, s_chunk;
+    int* piv = sp + m;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { s_bad = 0; s_base = 0; }
+    __syncthreads();
+    for (int q = tid; q < m; q += kComposeThreads) sp[q] = init ? q : pos[q];
+    for (int i = k0 + tid; i < k1; i += kComposeThreads) {
+        const int b = ipiv[i] - 1 - ipiv_minus;
+        if (b < i || b >= m) s_bad = 1;
+        piv[i - k0] = b;
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (tid == 0) {
+            *count = 0;
+            if (info) atomicExch(info, -1);
+            atomicExch(err, kErrBadPivot);
+        }
+        return;
+    }
+    if (tid == 0) {
+        for (int i = k0; i < k1; ++i) {
+            const int b = piv[i - k0];
+            if (b != i) {
+                const int t = sp[i];
+                sp[i] = sp[b];
+                sp[b] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int q0 = 0; q0 < m; q0 += kComposeThreads) {
+        const int q = q0 + tid;
+        const int s = q < m ? sp[q] : q;
+        if (q < m) pos[q] = s;
+        const bool moved = q < m && s != q;
+        const unsigned ball = __ballot_sync(0xffffffffu, moved);
+        const int within = __popc(ball & ((1u << lane) - 1u));
+        if (lane == 0) warp_tot[warp] = __popc(ball);
+        __syncthreads();
+        if (tid == 0) {
+            int run = 0;
+            for (int wv = 0; wv < kComposeThreads / 32; ++wv) {
+                const int t = warp_tot[wv];
+                warp_tot[wv] = run;
+                run += t;
+            }
+            s_chunk = run;
+        }
+        __syncthreads();
+        if (moved) {
+            const int o = s_base + warp_tot[warp] + within;
+            src[o] = s;
+            tgt[o] = q;
+        }
+        __syncthreads();
+        if (tid == 0) s_base += s_chunk;
+        __syncthreads();
+    }
     if (tid == 0) *count = s_base;
 }
 
@@ -437,12 +602,14 @@ void configure_getrf_kernels(hdbf_context* ctx)
                          (int)cap4);
     cudaFuncSetAttribute(apply_moves_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)cap4);
+    cudaFuncSetAttribute(compose_running_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)cap4);
     cudaGetLastError();
 }
 
 size_t getf2_coop_scratch_bytes()
 {
-    return align_up((size_t)(2 * kCoopMaxGrid * kSlotFloats) * sizeof(float), 256);
+    return align_up((size_t)(2 * kCoopMaxGrid * kSlotWords) * sizeof(unsigned long long), 256);
 }
 
 hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
@@ -452,7 +619,7 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     if (m <= 0 || w <= 0) return HDBF_STATUS_SUCCESS;
     if (w > kCoopMaxW) return HDBF_STATUS_INVALID_VALUE;
     HDBF_TRY(ensure_ws(ctx, 64));
-    float* scr = ws_coop(ctx);
+    unsigned long long* scr = reinterpret_cast<unsigned long long*>(ws_coop(ctx));
 
     // Grid: ~256 rows per CTA (panel_rows; measured fastest at n = 32768),
     // more when the slice would not fit in shared memory, at most one CTA per
@@ -469,7 +636,7 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     if (G < 1) G = 1;
     int rpc = (m + G - 1) / G;
     size_t smem = (size_t)rpc * w * sizeof(float);
-    if (smem > smem_cap) return HDBF_STATUS_NOT_SUPPORTED;
+    if (smem > smem_cap || rpc >= (int)kNoRow) return HDBF_STATUS_NOT_SUPPORTED;
     unsigned* epoch = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallEpoch);
     unsigned* done = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallDone);
     int* err = ctx->dev_small + kSmallErr;
@@ -497,6 +664,27 @@ hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_mi
     ProfScope prof(ctx, kClsCompose, 0.0, 4.0 * k + 8.0 * m);
     compose_swaps_kernel<<<1, kComposeThreads, use_smem ? smem : 0, ctx->stream>>>(
         ipiv, k, ipiv_minus, m, src, tgt, count, gperm, use_smem, info,
+        ctx->dev_small + kSmallErr);
+    ctx->launches++;
+    return last_cuda(ctx);
+}
+
+int compose_running_max_m(hdbf_context* ctx)
+{
+    const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
+    return (int)(cap / sizeof(int));  // block height + new swaps
+}
+
+hdbf_status compose_running(hdbf_context* ctx, const int* ipiv, int k0, int k1, int ipiv_minus,
+                            int m, int* pos, bool init, int* src, int* tgt, int* count, int* info)
+{
+    if (m <= 0) return HDBF_STATUS_SUCCESS;
+    if (m + (k1 - k0) > compose_running_max_m(ctx) || k0 < 0 || k1 < k0 || k1 > m)
+        return HDBF_STATUS_INVALID_VALUE;
+    ProfScope prof(ctx, kClsCompose, 0.0, 4.0 * (k1 - k0) + 12.0 * m);
+    const size_t smem = ((size_t)m + (size_t)(k1 - k0)) * sizeof(int);
+    compose_running_kernel<<<1, kComposeThreads, smem, ctx->stream>>>(
+        ipiv, k0, k1, ipiv_minus, m, pos, init ? 1 : 0, src, tgt, count, info,
         ctx->dev_small + kSmallErr);
     ctx->launches++;
     return last_cuda(ctx);

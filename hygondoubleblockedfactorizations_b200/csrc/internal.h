@@ -47,6 +47,10 @@ struct GraphEntry {
 };
 }  // namespace hdbf
 
+namespace hdbf {
+constexpr int kLaEvents = 33;  // 32 outer-update chunks per block + the join
+}
+
 struct hdbf_context {
     cudaStream_t stream = nullptr;
     int device = 0;
@@ -56,6 +60,15 @@ struct hdbf_context {
     int panel_mode = 0;   // hdbf_set_panel_kernel
     int panel_leaf = 128; // GETRF panel recursion leaf width (32, 64 or 128)
     int panel_rows = 256; // target rows per CTA of the grid-wide panel kernel
+    // GETRF look-ahead (hdbf_set_lookahead): the panel chain of an outer block
+    // runs on a high-priority internal stream while the caller's stream still
+    // applies the outer update chunk by chunk; la_ev[c] marks chunk c done and
+    // la_ev[kLaEvents - 1] joins the panel chain back.
+    int lookahead = 1;
+    cudaStream_t la_stream = nullptr;
+    cudaEvent_t la_ev[hdbf::kLaEvents] = {};
+    bool la_used = false;    // the graph being captured forked onto la_stream
+    bool no_skinny = false;  // keep GEMMs off the shared split-K scratch
     // Workspace arena (grown on demand outside stream capture).
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -127,18 +140,20 @@ void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st);
 // Workspace layout for problems of order <= n (byte offsets):
 //   coop  panel-kernel exchange slots (fixed size, offset 0)
 //   inv   inverted 64x64 diagonal blocks, ceil(n/64)*4096 floats
+//   perm  running composed row permutation of a GETRF outer block, n ints
 //   src, tgt, gperm  composed row moves / permutation scratch, n ints each
 //   temp  column-tiled swap buffer, 64*n floats
 //   skinny  split-K partial sums of the skinny GEMM, 256*n floats
 //   wave  wavefront-solve row-major x copy (32 columns) and its flags
 struct WsLayout {
-    size_t coop, inv, src, tgt, gperm, temp, skinny, wave, total;
+    size_t coop, inv, perm, src, tgt, gperm, temp, skinny, wave, total;
 };
 WsLayout ws_layout(int n);
 // Guarantee the layout for order n (grows the arena outside stream capture).
 hdbf_status ensure_ws(hdbf_context* ctx, int n);
 float* ws_coop(hdbf_context* ctx);
 float* ws_inv(hdbf_context* ctx);
+int* ws_perm(hdbf_context* ctx);
 int* ws_src(hdbf_context* ctx);
 int* ws_tgt(hdbf_context* ctx);
 int* ws_gperm(hdbf_context* ctx);
@@ -239,6 +254,16 @@ int configure_cluster_panel(hdbf_context* ctx);
 hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_minus, int m,
                           int* src, int* tgt, int* count, int* gperm, int* info);
 // A[tgt[i], c] = old A[src[i], c] for c < ncols, i < *count (<= max_moves).
+// Running composition: pos (m ints, row i of the block holds original row
+// pos[i]) is reset to the identity when init is set, then the LAPACK swaps
+// ipiv[k0, k1) (1-based, minus ipiv_minus gives rows local to the block) are
+// replayed into it, and every i with pos[i] != i becomes a move (pos[i] -> i),
+// in increasing i.  Fails (count 0, info -1) on a pivot outside [i, m).
+hdbf_status compose_running(hdbf_context* ctx, const int* ipiv, int k0, int k1, int ipiv_minus,
+                            int m, int* pos, bool init, int* src, int* tgt, int* count,
+                            int* info);
+// Largest block height + swap count compose_running holds in shared memory.
+int compose_running_max_m(hdbf_context* ctx);
 hdbf_status apply_moves(hdbf_context* ctx, float* A, long long lda, int ncols,
                         const int* src, const int* tgt, const int* count, int max_moves,
                         float* temp, long long temp_cols);
@@ -289,6 +314,8 @@ hdbf_status trsm_rlt(hdbf_context* ctx, int rows, int cols, const float* L, long
                      float* B, long long ldb);
 hdbf_status trsm_llu(hdbf_context* ctx, int rows, int cols, const float* L, long long ldl,
                      float* B, long long ldb);
+// Create the look-ahead stream and events (outside stream capture).
+hdbf_status ensure_lookahead(hdbf_context* ctx);
 hdbf_status syrk_lower(hdbf_context* ctx, int n, int k, const float* A, long long lda,
                        float* C, long long ldc);
 struct GetrfWs {

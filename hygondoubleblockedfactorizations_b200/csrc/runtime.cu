@@ -88,6 +88,8 @@ WsLayout ws_layout(int n)
     off += getf2_coop_scratch_bytes();
     L.inv = off;  // whole 64x64 blocks, the last one padded
     off += align_up((size_t)(n + 63) / 64 * 64 * 64 * sizeof(float), 256);
+    L.perm = off;
+    off += align_up((size_t)n * sizeof(int), 256);
     L.src = off;
     off += align_up((size_t)n * sizeof(int), 256);
     L.tgt = off;
@@ -132,6 +134,34 @@ float* ws_inv(hdbf_context* ctx)
 {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).inv);
 }
+int* ws_perm(hdbf_context* ctx)
+{
+    return reinterpret_cast<int*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).perm);
+}
+
+hdbf_status ensure_lookahead(hdbf_context* ctx)
+{
+    if (ctx->la_stream) return HDBF_STATUS_SUCCESS;
+    if (ctx->capturing) return HDBF_STATUS_NOT_SUPPORTED;
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    for (int i = 0; i < kLaEvents; ++i) {
+        if (cudaEventCreateWithFlags(&ctx->la_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            for (int j = 0; j < i; ++j) cudaEventDestroy(ctx->la_ev[j]);
+            cudaStreamDestroy(s);
+            return HDBF_STATUS_CUDA_ERROR;
+        }
+    }
+    ctx->la_stream = s;
+    return HDBF_STATUS_SUCCESS;
+}
+
 int* ws_src(hdbf_context* ctx)
 {
     return reinterpret_cast<int*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).src);
@@ -236,6 +266,7 @@ hdbf_status graph_capture_begin(hdbf_context* ctx, cudaStream_t* saved)
     *saved = ctx->stream;
     ctx->stream = ctx->cap_stream;
     ctx->capturing = true;
+    ctx->la_used = false;
     return HDBF_STATUS_SUCCESS;
 }
 
@@ -264,7 +295,11 @@ hdbf_status graph_capture_end(hdbf_context* ctx, cudaStream_t saved, hdbf_status
         return body_status;
     }
     cudaGraphExec_t exec = nullptr;
-    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    // A look-ahead graph keeps the priorities its kernel nodes were captured
+    // with (the panel chain's high-priority stream), not the launch stream's.
+    const unsigned long long iflags = ctx->la_used ? cudaGraphInstantiateFlagUseNodePriority : 0;
+    ctx->la_used = false;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, iflags);
     cudaGraphDestroy(graph);
     if (ie != cudaSuccess) {
         cudaGetLastError();
@@ -343,6 +378,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
         const int v = std::atoi(pr);
         if (v >= 64 && v <= 4096) ctx->panel_rows = v;
     }
+    if (const char* la = std::getenv("HDBF_LOOKAHEAD")) ctx->lookahead = std::atoi(la) != 0;
     configure_tc_kernels(ctx);
     configure_trsm_block_kernels(ctx);
     configure_solve_kernels(ctx);
@@ -361,6 +397,11 @@ hdbf_status hdbf_destroy(hdbf_handle h)
     graph_cache_clear(h);
     destroy_records(h->prof);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    if (h->la_stream) {
+        cudaStreamSynchronize(h->la_stream);
+        for (int i = 0; i < kLaEvents; ++i) cudaEventDestroy(h->la_ev[i]);
+        cudaStreamDestroy(h->la_stream);
+    }
     if (h->ws) cudaFree(h->ws);
     if (h->dev_small) cudaFree(h->dev_small);
     if (h->mix) cudaFree(h->mix);
@@ -433,6 +474,7 @@ hdbf_status hdbf_check_device_errors(hdbf_handle h)
         unsigned epoch = 0;
         cudaMemcpy(&epoch, h->dev_small + kSmallEpoch, sizeof(int), cudaMemcpyDeviceToHost);
         cudaMemset(h->dev_small, 0, kSmallInts * sizeof(int));
+        if (h->ws) cudaMemset(h->ws, 0, std::min(getf2_coop_scratch_bytes(), h->ws_bytes));
         epoch += 2;
         cudaMemcpy(h->dev_small + kSmallEpoch, &epoch, sizeof(int), cudaMemcpyHostToDevice);
         cudaDeviceSynchronize();
@@ -570,6 +612,14 @@ hdbf_status hdbf_set_panel_kernel(hdbf_handle h, int mode)
     if (mode < 0 || mode > 2) return HDBF_STATUS_INVALID_VALUE;
     if (mode != h->panel_mode) graph_cache_clear(h);
     h->panel_mode = mode;
+    return HDBF_STATUS_SUCCESS;
+}
+
+hdbf_status hdbf_set_lookahead(hdbf_handle h, int enabled)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    if ((enabled != 0) != (h->lookahead != 0)) graph_cache_clear(h);
+    h->lookahead = enabled != 0;
     return HDBF_STATUS_SUCCESS;
 }
 

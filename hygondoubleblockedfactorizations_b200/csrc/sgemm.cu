@@ -224,7 +224,7 @@ hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, in
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
     if (!A || !B || !C) return HDBF_STATUS_INVALID_VALUE;
     if (lower_only && mode != kNT) return HDBF_STATUS_INVALID_VALUE;
-    if (!lower_only && N <= 32 && M >= 4 * N && M >= 256)
+    if (!lower_only && !ctx->no_skinny && N <= 32 && M >= 4 * N && M >= 256)
         return sgemm_skinny(ctx, mode == kNT ? 0 : mode == kNN ? 1 : 2, M, N, K, A, lda, B, ldb,
                             C, ldc);
     const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);

@@ -12,7 +12,10 @@ also records the call's profiled CUDA graph), then ``reps`` profiled calls, and 
 one JSON line: total time, TFLOP/s (n^3/3 or 2n^3/3) and, per kernel class,
 launches, milliseconds, share of the device time and TFLOP/s or GB/s.
 ``--panel`` selects the GETRF panel kernel (0 automatic, 1 grid-wide,
-2 cluster).  Mixed precisions use ``hdbf_spotrf_mixed`` / ``hdbf_sgetrf_mixed``
+2 cluster); ``--batched`` runs the FP32 GETRF through
+``double_blocked_getrf_batched_pivot`` (iterative outer TRSM, as the
+benchmark does) instead of ``double_blocked_getrf``, and ``--lookahead 0|1``
+sets the handle's GETRF look-ahead.  Mixed precisions use ``hdbf_spotrf_mixed`` / ``hdbf_sgetrf_mixed``
 with panel width ``--inner``.
 """
 from __future__ import annotations
@@ -37,23 +40,41 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--panel", type=int, default=None)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--batched", action="store_true")
+    ap.add_argument("--lookahead", type=int, default=None)
     a = ap.parse_args(argv)
 
     P = ctypes.c_void_p
     h = Handle(torch.cuda.current_stream().cuda_stream)
     if a.panel is not None:
         h.set_panel_kernel(a.panel)
+    if a.lookahead is not None:
+        h.set_lookahead(bool(a.lookahead))
     n = a.n
     A0 = _matrix(torch, h, a.op, n, a.seed)
     A = torch.empty_like(A0)
     ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    if a.batched:
+        import numpy as np
+
+        from . import WorkspacePivot
+        tile = 64
+        keep = [torch.zeros(n, dtype=torch.int32, device="cuda"),
+                torch.zeros(n, dtype=torch.int32, device="cuda"),
+                torch.zeros(n * tile, dtype=torch.float32, device="cuda")]
+        host = [np.zeros(n, np.int32) for _ in range(4)]
+        ws = WorkspacePivot(keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr(),
+                            *[x.ctypes.data for x in host], n, tile)
 
     def run():
         A.copy_(A0)
         if a.precision == "fp32" and a.op == "potrf":
             call("double_blocked_potrf_kblocked_syrk", h.ptr, P(A.data_ptr()), n, n, a.outer,
                  a.inner, 0, P(info.data_ptr()))
+        elif a.precision == "fp32" and a.batched:
+            call("double_blocked_getrf_batched_pivot", h.ptr, P(A.data_ptr()), n, n, a.outer,
+                 a.inner, 1, 0, 0, P(ipiv.data_ptr()), P(info.data_ptr()), ctypes.byref(ws))
         elif a.precision == "fp32":
             call("double_blocked_getrf", h.ptr, P(A.data_ptr()), n, n, a.outer, a.inner, 0, 0,
                  P(ipiv.data_ptr()), P(info.data_ptr()))
@@ -90,7 +111,7 @@ def main(argv=None):
                      "tflops": round(fl / (t / 1e3) / 1e12, 3) if fl and t else None,
                      "gbs": round(by / (t / 1e3) / 1e9, 1) if by and t else None}
     out = {"op": a.op, "precision": a.precision, "n": n, "outer": a.outer, "inner": a.inner,
-           "panel": a.panel, "ms": round(ms, 3), "tflops": round(flops / (ms / 1e3) / 1e12, 3),
+           "panel": a.panel, "batched": a.batched, "lookahead": a.lookahead, "ms": round(ms, 3), "tflops": round(flops / (ms / 1e3) / 1e12, 3),
            "info": int(info.item()), "device_errors": h.device_errors(), "stages": stages}
     print(json.dumps(out), flush=True)
     return out

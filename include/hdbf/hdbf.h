@@ -98,6 +98,18 @@ hdbf_status hdbf_set_graph_mode(hdbf_handle handle, int enabled);
  * kernel aims to hold. */
 hdbf_status hdbf_set_panel_kernel(hdbf_handle handle, int mode);
 
+/* Look-ahead in the double-blocked GETRF entry points with batched pivoting
+ * or without pivoting (default on; HDBF_LOOKAHEAD=0 turns a new handle's
+ * off).  The outer TRSM of the next outer block runs whole; its outer GEMM
+ * then runs in column chunks of the inner panel width on the handle's
+ * stream, while the inner panels of that block are factored, each as soon as
+ * its chunk is updated, on a high-priority internal stream that joins the
+ * handle's stream again at the end of the block.  Row interchanges of the
+ * block's panels reach each later inner panel, composed, just before its
+ * inner update.  Pivots and factors are the same as without look-ahead.
+ * double_blocked_getrf (immediate pivoting) always runs serially. */
+hdbf_status hdbf_set_lookahead(hdbf_handle handle, int enabled);
+
 /* Per-launch event profiling of this library's kernels on the handle's
  * stream.  Between begin and end every launch is bracketed by CUDA events;
  * end synchronises the stream and returns, per kernel class (see

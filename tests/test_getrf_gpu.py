@@ -270,3 +270,89 @@ def test_panel_kernels_agree_bitwise_large(hd, handle, torch_cuda):
     PA = A[torch.from_numpy(perm).cuda()]
     r = (torch.linalg.matrix_norm(PA - L @ U) / torch.linalg.matrix_norm(A)).item()
     assert r / (n * 2.0 ** -23) <= BOUND, r
+
+
+@pytest.mark.parametrize("n,outer,inner,mode,tblock,mtile", [
+    (3072, 1024, 256, 0, 0, 0),      # three outer blocks, four chunks each
+    (2500, 768, 128, 1, 384, 500),   # ragged last block, iterative outer TRSM
+    (4096, 2048, 32, 0, 0, 0),       # 64 inner panels per block: chunks of two panels
+])
+def test_lookahead_bitwise_batched(hd, handle, torch_cuda, n, outer, inner, mode, tblock, mtile):
+    """Look-ahead (panel chain on the internal stream, outer GEMM in chunks,
+    running composed interchanges) moves the same data and runs the same
+    arithmetic as the serial schedule: factors and pivots are bit-identical,
+    graph capture included (the second call of each replays its graph)."""
+    import ctypes
+    G = oracle.general_uniform(n, 3)
+    ws, keep = make_ws(torch_cuda, n, tile=64)
+    out = {}
+    try:
+        for la in (0, 1):
+            handle.set_lookahead(la)
+            for rep in range(2):
+                dA, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G,
+                                               "double_blocked_getrf_batched_pivot", outer=outer,
+                                               inner=inner, mode=mode, tblock=tblock, mtile=mtile,
+                                               ws=ctypes.byref(ws))
+                handle.check()
+                assert info == 0 and handle.device_errors() == 0
+                out[(la, rep)] = (dA.clone(), ipiv)
+    finally:
+        handle.set_lookahead(1)
+    for k in out:
+        assert torch_cuda.equal(out[k][0], out[(0, 0)][0]), k
+        np.testing.assert_array_equal(out[k][1], out[(0, 0)][1])
+    assert_pivots_match(G, out[(1, 0)][1], oracle.lapack_sgetrf(G)[1], "host sgetrf")
+    LU = host2d(out[(1, 0)][0], n, n, n)
+    assert getrf_check(LU[:n], G, out[(1, 0)][1]) <= BOUND
+
+
+def test_lookahead_npvt_and_ragged(hd, handle, torch_cuda):
+    """No-pivot look-ahead is bit-identical to the serial schedule; a last
+    outer block narrower than 32 columns (the serial path may take the
+    split-K skinny GEMM there) still factors to the residual bound."""
+    import ctypes
+    n = 2048
+    G = oracle.general_uniform(n, 5) + np.float32(n) * np.eye(n, dtype=np.float32)
+    res = {}
+    try:
+        for la in (0, 1):
+            handle.set_lookahead(la)
+            dA, LU, _, info = run_getrf(hd, handle, torch_cuda, G, "double_blocked_getrf_npvt",
+                                        outer=512, inner=128)
+            handle.check()
+            assert info == 0
+            res[la] = dA.clone()
+        assert torch_cuda.equal(res[0], res[1])
+        assert getrf_check(host2d(res[1], n, n, n)[:n], G, None, pivoting=False) <= BOUND
+        n2 = 1024 + 20
+        G2 = oracle.general_uniform(n2, 6)
+        ws, keep = make_ws(torch_cuda, n2)
+        handle.set_lookahead(1)
+        _, LU2, ipiv2, info2 = run_getrf(hd, handle, torch_cuda, G2,
+                                         "double_blocked_getrf_batched_pivot", outer=512,
+                                         inner=128, ws=ctypes.byref(ws))
+        handle.check()
+        assert info2 == 0
+        assert_pivots_match(G2, ipiv2, oracle.lapack_sgetrf(G2)[1], "host sgetrf")
+        assert getrf_check(LU2[:n2], G2, ipiv2) <= BOUND
+    finally:
+        handle.set_lookahead(1)
+
+
+def test_panel_exchange_after_narrow_launch(hd, handle, torch_cuda):
+    """Grid-wide panel launches of 65..67 columns followed by further launches
+    (the exchange words of one launch must never be taken for the next's):
+    pivots follow host sgetrf and the factors meet the residual bound."""
+    handle.set_panel_kernel(1)
+    try:
+        for n, nb in ((1090, 1024), (2115, 1024), (3000, 67)):
+            G = oracle.general_uniform(n, 11)
+            _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G,
+                                          "blocked_right_looking_getrf", outer=nb)
+            handle.check()
+            assert info == 0 and handle.device_errors() == 0
+            assert_pivots_match(G, ipiv, oracle.lapack_sgetrf(G)[1], "host sgetrf")
+            assert getrf_check(LU[:n], G, ipiv) <= BOUND
+    finally:
+        handle.set_panel_kernel(0)
