@@ -44,9 +44,9 @@ void* workspace(hdbf_context* ctx, size_t bytes, hdbf_status* st)
     }
     ctx->ws_bytes = want;
     ctx->ws_n = fitting_order(want);
-    // The panel kernel's exchange slots must never hold a stale sequence
-    // number that matches a live one: clear them on every (re)allocation.
-    cudaMemset(ctx->ws, 0, getf2_coop_scratch_bytes() < want ? getf2_coop_scratch_bytes() : want);
+    // Exchange slots must never hold a stale tag that matches a live one:
+    // clear the whole arena on every (re)allocation.
+    cudaMemset(ctx->ws, 0, want);
     cudaDeviceSynchronize();
     return ctx->ws;
 }
@@ -474,7 +474,7 @@ hdbf_status hdbf_check_device_errors(hdbf_handle h)
         unsigned epoch = 0;
         cudaMemcpy(&epoch, h->dev_small + kSmallEpoch, sizeof(int), cudaMemcpyDeviceToHost);
         cudaMemset(h->dev_small, 0, kSmallInts * sizeof(int));
-        if (h->ws) cudaMemset(h->ws, 0, std::min(getf2_coop_scratch_bytes(), h->ws_bytes));
+        if (h->ws) cudaMemset(h->ws, 0, h->ws_bytes);  // exchange words with the counters
         epoch += 2;
         cudaMemcpy(h->dev_small + kSmallEpoch, &epoch, sizeof(int), cudaMemcpyHostToDevice);
         cudaDeviceSynchronize();

@@ -206,3 +206,29 @@ def test_batched_syrk_and_trsm_mixed(hd, handle, torch_cuda):
     want = np.linalg.solve(L.astype(np.float64), Bm.astype(np.float64).T).T
     got = host2d(dB, n, n, m)
     assert np.abs(got - want).max() <= 2e-2 * np.abs(want).max()
+
+
+def test_wave_solve_repeated_launches(hd, handle, torch_cuda):
+    """Wavefront solves of different orders back to back: the ready flags and
+    solution copies an earlier (larger) launch left behind are never taken
+    for the current ones; the repeated results are bit-identical and match
+    the FP64 solution."""
+    out = {}
+    for rep in range(2):
+        for n, nrhs in ((4096, 16), (700, 5), (4096, 16), (1500, 32)):
+            A = oracle.spd_gram(n, 9)
+            L = np.linalg.cholesky(A.astype(np.float64)).astype(np.float32)
+            B = np.random.default_rng(n + nrhs).standard_normal((n, nrhs)).astype(np.float32)
+            dL = dev(torch_cuda, L)
+            dB = dev(torch_cuda, B)
+            st = hd.call("hdbf_spotrs", handle.ptr, ptr(dL), n, n, nrhs, ptr(dB), n)
+            torch_cuda.cuda.synchronize()
+            assert st == 0 and handle.device_errors() == 0
+            X = host2d(dB, n, n, nrhs)
+            if (n, nrhs) in out:
+                np.testing.assert_array_equal(X, out[(n, nrhs)])
+            else:
+                want = np.linalg.solve(L.astype(np.float64) @ L.astype(np.float64).T,
+                                       B.astype(np.float64))
+                assert np.abs(X - want).max() <= 1e-4 * np.abs(want).max()
+                out[(n, nrhs)] = X
