@@ -315,6 +315,102 @@ def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
     return out
 
 
+def fp64_case(torch, hd, handle, n=8192, reps=2):
+    """FP64 twins at n=8192: double_blocked_potrf_double (nb 2048, b 256) and
+    double_blocked_getrf_double_batched_pivot (nb 2048, b 256, iterative outer
+    TRSM) on the bench's input families drawn in FP32 by the seeded generator
+    and widened to FP64 (SPD G G^T/n + I, general U[-1,1)).  Device time per
+    call with CUDA events (mean of `reps` after one warm-up, the input restored
+    from a pristine copy outside the timed region); TFLOP/s with n^3/3 and
+    2n^3/3 against the nominal FP64 FMA peak; FP64 residuals
+    ||A - LL^T||_F / (||A||_F n eps64) and ||PA - LU||_F / (||A||_F n eps64)."""
+    import ctypes
+
+    import numpy as np
+    P = ctypes.c_void_p
+    dev = torch.device("cuda")
+
+    def draw(seed):
+        x = torch.empty(n * n, dtype=torch.float32, device=dev)
+        hd.lib().hdbf_fill_uniform(handle.ptr, P(x.data_ptr()), n * n, seed, 0)
+        return x.view(n, n).t().double()  # column-major storage: element (r, c) at c*n + r
+
+    G = draw(0)
+    spd0 = (G @ G.t()) / n + torch.eye(n, dtype=torch.float64, device=dev)
+    spd0 = 0.5 * (spd0 + spd0.t())
+    gen0 = draw(1)
+    del G
+    # the library reads column-major: keep each matrix as the transpose's storage
+    spd_cm = spd0.t().contiguous()
+    gen_cm = gen0.t().contiguous()
+    A = torch.empty_like(spd_cm)
+    info = torch.zeros(2, dtype=torch.int32, device=dev)
+    ipiv = torch.zeros(n, dtype=torch.int32, device=dev)
+    tile = 16
+    keep = [torch.zeros(n, dtype=torch.int32, device=dev),
+            torch.zeros(n, dtype=torch.int32, device=dev),
+            torch.zeros(n * tile, dtype=torch.float64, device=dev)]
+    host = [np.zeros(n, np.int32) for _ in range(4)]
+    ws = hd.WorkspacePivot(keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr(),
+                           *[h.ctypes.data for h in host], n, tile)
+
+    def potrf():
+        hd.call("double_blocked_potrf_double", handle.ptr, P(A.data_ptr()), n, n, 2048, 256,
+                P(info.data_ptr()))
+
+    def getrf():
+        hd.call("double_blocked_getrf_double_batched_pivot", handle.ptr, P(A.data_ptr()), n, n,
+                2048, 256, 1, 0, 0, P(ipiv.data_ptr()), P(info.data_ptr() + 4), ctypes.byref(ws))
+
+    def timed(src, fn):
+        times = []
+        for r in range(reps + 1):
+            A.copy_(src)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if r > 0:
+                times.append(e0.elapsed_time(e1))
+        handle.check()
+        return sum(times) / len(times)
+
+    eps = 2.0 ** -52
+    ms_p = timed(spd_cm, potrf)
+    L = torch.tril(A.t())
+    res_p = float(torch.linalg.norm(spd0 - L @ L.t()) / torch.linalg.norm(spd0)) / (n * eps)
+    del L
+    ms_g = timed(gen_cm, getrf)
+    LU = A.t()
+    Lm = torch.tril(LU, -1) + torch.eye(n, dtype=torch.float64, device=dev)
+    Um = torch.triu(LU)
+    perm = np.arange(n)
+    piv = ipiv.cpu().numpy()
+    for i in range(n):
+        p = int(piv[i]) - 1
+        perm[i], perm[p] = perm[p], perm[i]
+    PA = gen0[torch.from_numpy(perm).to(dev)]
+    res_g = float(torch.linalg.norm(PA - Lm @ Um) / torch.linalg.norm(gen0)) / (n * eps)
+    infos = info.cpu().tolist()
+    props = torch.cuda.get_device_properties(0)
+    peak = props.multi_processor_count * 64 * 2 * 1965e6 / 1e12
+    tp = n ** 3 / 3.0 / (ms_p / 1e3) / 1e12
+    tg = 2.0 * n ** 3 / 3.0 / (ms_g / 1e3) / 1e12
+    return {"workload": f"n={n} double_blocked_potrf_double(nb 2048, b 256) + "
+                        "double_blocked_getrf_double_batched_pivot(nb 2048, b 256, iterative "
+                        "outer TRSM)",
+            "potrf_ms": round(ms_p, 3), "getrf_ms": round(ms_g, 3),
+            "potrf_tflops": round(tp, 3), "getrf_tflops": round(tg, 3),
+            "peak_tflops": round(peak, 2),
+            "peak_source": f"nominal: {props.multi_processor_count} SMs x 64 FP64 FMA/clk x 2 "
+                           "x 1965 MHz (no measured FP64 peak on this pool)",
+            "frac_potrf": round(tp / peak, 4), "frac_getrf": round(tg / peak, 4),
+            "scaled_residual": {"potrf": round(res_p, 4), "getrf": round(res_g, 4)},
+            "info": infos, "eps": "2^-52"}
+
+
 def batched_case(torch, hd, handle, reps=5):
     """The uneven batch in one persistent launch: 4096 SPD systems with
     n ~ U[16, 512] and 2048 general systems with n ~ U[32, 768] (seed 3), one
@@ -571,6 +667,13 @@ def run_ours(args, rank, world):
     if not args.skip_batched and world == 1:
         batched = batched_case(torch, hd, handle)
 
+    fp64 = None
+    if not args.skip_fp64 and world == 1:
+        try:
+            fp64 = fp64_case(torch, hd, handle)
+        except Exception as exc:  # reported in the line, never hides the FP32 result
+            fp64 = {"error": f"{type(exc).__name__}: {exc}"}
+
     total_flops = world * args.steps * (flops_potrf(n) + flops_getrf(n))
     value = total_flops / (ms_max / 1e3) / 1e12
     vs_baseline = None
@@ -625,7 +728,7 @@ def run_ours(args, rank, world):
            "getrf_tflops": round(flops_getrf(n) / (ms_getrf / 1e3) / 1e12, 3),
            "info": info, "gpu_launches": launches, "kernels": kernels,
            "roofline": roof, "clocks": clocks, "e2e": e2e, "mixed_ir": mixed,
-           "batched": batched}
+           "batched": batched, "fp64": fp64}
     return out, handle
 
 
@@ -640,6 +743,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-mixed", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

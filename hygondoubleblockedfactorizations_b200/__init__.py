@@ -102,6 +102,37 @@ _PROTOS = {
     "hdbf_batched_factor_solve": (c_int, [P, c_int, c_int, P, P, P, P, P, P, P, P, P]),
     "launch_mixed_gemm": (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_float, P, c_int, P,
                                  c_int, c_float, P, c_int]),
+    # FP64 twins (the reference's `_double` entry points)
+    "double_blocked_potrf_double": (None, [P, P, c_int, c_int, c_int, c_int, P]),
+    "double_blocked_potrf_double_dbtrsm": (None, [P, P, c_int, c_int, c_int, c_int, P]),
+    "double_blocked_potrf_double_kblocked_syrk":
+        (None, [P, P, c_int, c_int, c_int, c_int, c_int, P]),
+    "double_blocked_potrf_double_kblocked_syrk_adaptive_gemm":
+        (None, [P, P, c_int, c_int, c_int, c_int, c_int, P]),
+    "double_blocked_potrf_double_kblocked_syrk_adaptive_gemm_configured":
+        (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, P]),
+    "blocked_right_looking_potrf_double": (None, [P, P, c_int, c_int, c_int, P]),
+    "recursive_potrf_double": (None, [P, P, P, c_int, c_int, c_int, P]),
+    "double_blocked_getrf_double":
+        (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_int, P, P]),
+    "double_blocked_getrf_double_batched_pivot":
+        (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int, P, P, P]),
+    "double_blocked_getrf_npvt_double": (None, [P, P, c_int, c_int, c_int, c_int, P]),
+    "blocked_right_looking_getrf_double": (None, [P, P, c_int, c_int, c_int, P, P]),
+    "blocked_right_looking_getrf_npvt_double": (None, [P, P, c_int, c_int, c_int, P]),
+    "launch_apply_getrf_panel_pivots_double": (None, [P, c_int, c_int, c_int, c_int, P, P]),
+    "launch_apply_getrf_permutation_double":
+        (None, [P, c_int, c_int, P, P, c_int, P, c_int, P]),
+    "syrk_lower_update_double": (None, [P, c_int, c_int, P, c_int, P, c_int]),
+    "syrk_lower_update_kblocked_double": (None, [P, c_int, c_int, P, c_int, P, c_int, c_int]),
+    "recursive_syrk_parallel_double": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
+    "batched_syrk_bottom_up_double": (None, [P, P, P, c_int, P, c_int, c_int, c_int, c_int]),
+    "trsm_right_lower_transpose_double": (None, [P, c_int, c_int, P, c_int, P, c_int]),
+    "double_blocked_trsm_double": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int, c_int]),
+    "recursive_trsm_double": (None, [P, P, c_int, P, c_int, c_int, c_int, c_int]),
+    "gemm_nt_update_double": (None, [P, c_int, c_int, c_int, P, c_int, P, c_int, P, c_int]),
+    "gemm_nt_update_m_tiled_double":
+        (None, [P, c_int, c_int, c_int, P, c_int, P, c_int, P, c_int, c_int]),
     # kernels
     "launch_add_damping": (None, [P, c_int, c_int, c_float, P]),
     "launch_add_damping_double": (None, [P, c_int, c_int, c_double, P]),

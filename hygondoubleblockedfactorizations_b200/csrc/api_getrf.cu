@@ -12,7 +12,12 @@
 namespace hdbf {
 namespace {
 
-inline float* at(float* A, long long lda, int r, int c) { return A + (long long)c * lda + r; }
+template <class T>
+inline T* at(T* A, long long lda, int r, int c) { return A + (long long)c * lda + r; }
+
+// The row-move scratch of a workspace, in the factorization's scalar type.
+template <class T>
+inline T* ws_temp(const GetrfWs& ws) { return reinterpret_cast<T*>(ws.temp); }
 
 hdbf_status record(hdbf_context* ctx, hdbf_status st)
 {
@@ -33,7 +38,8 @@ __global__ void offset_pivots_kernel(int* p, int k, int delta)
 
 // Compose the swaps ipiv[0..k) (1-based, minus `minus` gives rows local to
 // A(row0:n, :)) and apply them to columns [c0, c0+nc) of rows row0..n.
-hdbf_status permute_cols(hdbf_context* ctx, const GetrfWs& ws, float* A, long long lda, int n,
+template <class T>
+hdbf_status permute_cols(hdbf_context* ctx, const GetrfWs& ws, T* A, long long lda, int n,
                          int row0, const int* ipiv, int k, int minus, int* info,
                          const int* col_begin, const int* col_count, int ranges)
 {
@@ -47,14 +53,15 @@ hdbf_status permute_cols(hdbf_context* ctx, const GetrfWs& ws, float* A, long lo
     for (int r = 0; r < ranges; ++r)
         if (col_count[r] > 0)
             HDBF_TRY(apply_moves(ctx, at(A, lda, row0, col_begin[r]), lda, col_count[r], ws.src,
-                                 ws.tgt, ws.count, max_moves, ws.temp, ws.temp_cols));
+                                 ws.tgt, ws.count, max_moves, ws_temp<T>(ws), ws.temp_cols));
     return HDBF_STATUS_SUCCESS;
 }
 
 // L11^{-1} applied to B (rows x cols), direct or in trsm_block row blocks
 // (src/getrf/getrf_pivot_internal.h:64-110).
-hdbf_status trsm_llu_mode(hdbf_context* ctx, int rows, int cols, float* L, long long ldl,
-                          float* B, long long ldb, bool iterative, int block)
+template <class T>
+hdbf_status trsm_llu_mode(hdbf_context* ctx, int rows, int cols, T* L, long long ldl,
+                          T* B, long long ldb, bool iterative, int block)
 {
     if (!iterative || block <= 0 || rows <= block) return trsm_llu(ctx, rows, cols, L, ldl, B, ldb);
     for (int r = 0; r < rows; r += block) {
@@ -62,7 +69,7 @@ hdbf_status trsm_llu_mode(hdbf_context* ctx, int rows, int cols, float* L, long 
         HDBF_TRY(trsm_llu(ctx, dr, cols, at(L, ldl, r, r), ldl, B + r, ldb));
         const int tr = rows - r - dr;
         if (tr > 0)
-            HDBF_TRY(sgemm_sub(ctx, true, false, tr, cols, dr, at(L, ldl, r + dr, r), ldl, B + r,
+            HDBF_TRY(gemm_sub(ctx, true, false, tr, cols, dr, at(L, ldl, r + dr, r), ldl, B + r,
                                ldb, B + r + dr, ldb));
     }
     return HDBF_STATUS_SUCCESS;
@@ -70,13 +77,14 @@ hdbf_status trsm_llu_mode(hdbf_context* ctx, int rows, int cols, float* L, long 
 
 // C -= L * U in row chunks (inner GEMM M-tiling,
 // src/getrf/getrf_batched_pivot_internal.h:285-323).
-hdbf_status gemm_nn_rows(hdbf_context* ctx, int rows, int cols, int k, const float* L,
-                         long long ldl, const float* U, long long ldu, float* C, long long ldc,
+template <class T>
+hdbf_status gemm_nn_rows(hdbf_context* ctx, int rows, int cols, int k, const T* L,
+                         long long ldl, const T* U, long long ldu, T* C, long long ldc,
                          int m_tile)
 {
     const int tile = m_tile > 0 ? m_tile : std::max(rows, 1);
     for (int r = 0; r < rows; r += tile)
-        HDBF_TRY(sgemm_sub(ctx, true, false, std::min(tile, rows - r), cols, k, L + r, ldl, U,
+        HDBF_TRY(gemm_sub(ctx, true, false, std::min(tile, rows - r), cols, k, L + r, ldl, U,
                            ldu, C + r, ldc));
     return HDBF_STATUS_SUCCESS;
 }
@@ -114,7 +122,8 @@ struct NoSkinny {
 // before its inner update (instead of one permutation per panel), because
 // the outer GEMM may still be writing those columns; the composition is kept
 // running across the block's panels, and the data movement is the same.
-hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer_nb,
+template <class T>
+hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
                           int inner_nb, bool iterative_outer, int trsm_block,
                           int inner_gemm_m_tile, int* ipiv, int* info, PivotMode mode,
                           const getrf_batched_pivot_workspace* user_ws)
@@ -126,7 +135,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
         return last_cuda(ctx);
     }
     GetrfWs ws;
-    HDBF_TRY(getrf_workspace(ctx, n, &ws));
+    HDBF_TRY(getrf_workspace(ctx, ws_order<T>(n), &ws));
     if (mode == PivotMode::Batched && user_ws) {
         ws.src = user_ws->device_sources;
         ws.tgt = user_ws->device_targets;
@@ -137,7 +146,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
     if (inner_nb <= 0) inner_nb = outer_nb;
     inner_nb = std::min(inner_nb, outer_nb);
     const bool piv = mode != PivotMode::None;
-    bool la = ctx->lookahead && mode != PivotMode::Immediate && n > outer_nb &&
+    bool la = sizeof(T) == 4 && ctx->lookahead && mode != PivotMode::Immediate && n > outer_nb &&
               n + inner_nb <= compose_running_max_m(ctx);
     if (la && !ctx->la_stream) {
         // The stream and events are created outside any capture.
@@ -149,7 +158,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
         }
     }
     const std::vector<long long> key = {
-        10 + (int)mode, (long long)A, lda, n, outer_nb, inner_nb, iterative_outer, trsm_block,
+        10 + (int)mode + type_tag<T>(), (long long)A, lda, n, outer_nb, inner_nb, iterative_outer, trsm_block,
         inner_gemm_m_tile, (long long)ipiv, (long long)info, (long long)ws.src, (long long)ws.tgt,
         (long long)ws.temp, ws.temp_cols, la ? 1 : 0};
     return run_graph(ctx, key, [&]() -> hdbf_status {
@@ -192,8 +201,8 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
                                              n - outer, ws_perm(ctx), inner == outer, ws.src,
                                              ws.tgt, ws.count, info));
                     HDBF_TRY(apply_moves(ctx, at(A, lda, outer, next), lda, nsz, ws.src, ws.tgt,
-                                         ws.count, std::min(n - outer, 2 * hist), ws.temp,
-                                         ws.temp_cols));
+                                         ws.count, std::min(n - outer, 2 * hist),
+                                         ws_temp<T>(ws), ws.temp_cols));
                 }
                 HDBF_TRY(trsm_llu(ctx, hist, nsz, at(A, lda, outer, outer), lda,
                                   at(A, lda, outer, next), lda));
@@ -246,13 +255,13 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
                 NoSkinny ns(ctx);  // the panel chain may use the split-K scratch
                 for (int c0 = 0; c0 < nsz; c0 += chunk_w) {
                     const int cw = std::min(chunk_w, nsz - c0);
-                    HDBF_TRY(sgemm_sub(ctx, true, false, n - next, cw, next, at(A, lda, next, 0),
+                    HDBF_TRY(gemm_sub(ctx, true, false, n - next, cw, next, at(A, lda, next, 0),
                                        lda, at(A, lda, 0, next + c0), lda,
                                        at(A, lda, next, next + c0), lda));
                     cudaEventRecord(ctx->la_ev[nchunks++], main_s);
                 }
             } else {
-                HDBF_TRY(sgemm_sub(ctx, true, false, n - next, nsz, next, at(A, lda, next, 0), lda,
+                HDBF_TRY(gemm_sub(ctx, true, false, n - next, nsz, next, at(A, lda, next, 0), lda,
                                    at(A, lda, 0, next), lda, at(A, lda, next, next), lda));
             }
         }
@@ -262,7 +271,8 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, float* A, int lda, int n, int outer
 }
 
 // Blocked right-looking LU (src/getrf/blocked_getrf.cpp:15-71).
-hdbf_status getrf_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, int* ipiv,
+template <class T>
+hdbf_status getrf_rl_impl(hdbf_context* ctx, T* A, int lda, int n, int nb, int* ipiv,
                           int* info, bool piv)
 {
     if (bad_matrix(A, lda, n)) return HDBF_STATUS_INVALID_VALUE;
@@ -272,9 +282,9 @@ hdbf_status getrf_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, i
         return last_cuda(ctx);
     }
     GetrfWs ws;
-    HDBF_TRY(getrf_workspace(ctx, n, &ws));
+    HDBF_TRY(getrf_workspace(ctx, ws_order<T>(n), &ws));
     if (nb <= 0) nb = n;
-    const std::vector<long long> key = {20 + (int)piv, (long long)A, lda, n, nb, (long long)ipiv,
+    const std::vector<long long> key = {20 + (int)piv + type_tag<T>(), (long long)A, lda, n, nb, (long long)ipiv,
                                         (long long)info};
     return run_graph(ctx, key, [&]() -> hdbf_status {
     if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
@@ -291,7 +301,7 @@ hdbf_status getrf_rl_impl(hdbf_context* ctx, float* A, int lda, int n, int nb, i
         }
         if (tr > 0) {
             HDBF_TRY(trsm_llu(ctx, psz, tr, at(A, lda, p, p), lda, at(A, lda, p, next), lda));
-            HDBF_TRY(sgemm_sub(ctx, true, false, tr, tr, psz, at(A, lda, next, p), lda,
+            HDBF_TRY(gemm_sub(ctx, true, false, tr, tr, psz, at(A, lda, next, p), lda,
                                at(A, lda, p, next), lda, at(A, lda, next, next), lda));
         }
     }
@@ -399,6 +409,90 @@ void launch_apply_getrf_permutation(float* A, int lda, int column_count, const i
     hdbf_context* ctx = launcher_context(stream);
     if (!ctx) return;
     // The move count is a host value here; stage it into the device word.
+    int* cnt = ctx->dev_small + kSmallMoveCount + 1;
+    cudaMemcpyAsync(cnt, &move_count, sizeof(int), cudaMemcpyHostToDevice, stream);
+    apply_moves(ctx, A, lda, column_count, sources, targets, cnt, move_count, temporary,
+                column_tile);
+}
+
+// ------------------------------------------------------------ FP64 twins
+// The reference's `_double` LU entry points: the same drivers instantiated
+// for double on this library's FP64 kernels (fp64.cu).
+
+void double_blocked_getrf_double(hdbf_handle h, double* A, int lda, int n, int outer_nb,
+                                 int inner_nb, getrf_outer_trsm_mode outer_trsm_mode,
+                                 int trsm_block, int* ipiv, int* info)
+{
+    if (!h) return;
+    record(h, getrf_db_impl(h, A, lda, n, outer_nb, inner_nb,
+                            outer_trsm_mode == getrf_outer_trsm_iterative, trsm_block, 0, ipiv,
+                            info, PivotMode::Immediate, nullptr));
+}
+
+void double_blocked_getrf_double_batched_pivot(hdbf_handle h, double* A, int lda, int n,
+                                               int outer_nb, int inner_nb,
+                                               getrf_outer_trsm_mode outer_trsm_mode,
+                                               int trsm_block, int inner_gemm_m_tile, int* ipiv,
+                                               int* info, getrf_batched_pivot_workspace* workspace)
+{
+    if (!h) return;
+    if (!batched_ws_valid(workspace, n)) {
+        if (info) cudaMemsetAsync(info, 0xff, sizeof(int), h->stream);
+        record(h, HDBF_STATUS_INVALID_VALUE);
+        return;
+    }
+    record(h, getrf_db_impl(h, A, lda, n, outer_nb, inner_nb,
+                            outer_trsm_mode == getrf_outer_trsm_iterative, trsm_block,
+                            inner_gemm_m_tile, ipiv, info, PivotMode::Batched, workspace));
+}
+
+void double_blocked_getrf_npvt_double(hdbf_handle h, double* A, int lda, int n, int nb, int b,
+                                      int* info)
+{
+    if (!h) return;
+    record(h, getrf_db_impl(h, A, lda, n, nb, b, false, 0, 0, nullptr, info, PivotMode::None,
+                            nullptr));
+}
+
+void blocked_right_looking_getrf_double(hdbf_handle h, double* A, int lda, int n, int nb,
+                                        int* ipiv, int* info)
+{
+    if (!h) return;
+    record(h, getrf_rl_impl(h, A, lda, n, nb, ipiv, info, true));
+}
+
+void blocked_right_looking_getrf_npvt_double(hdbf_handle h, double* A, int lda, int n, int nb,
+                                             int* info)
+{
+    if (!h) return;
+    record(h, getrf_rl_impl(h, A, lda, n, nb, nullptr, info, false));
+}
+
+void launch_apply_getrf_panel_pivots_double(double* A, int lda, int n, int panel,
+                                            int panel_size, int* pivots, cudaStream_t stream)
+{
+    if (!A || !pivots || panel_size <= 0 || n <= 0) return;
+    hdbf_context* ctx = launcher_context(stream);
+    if (!ctx) return;
+    GetrfWs ws;
+    if (getrf_workspace(ctx, ws_order<double>(n), &ws) != HDBF_STATUS_SUCCESS) return;
+    const int next = panel + panel_size;
+    const int cb[2] = {0, next};
+    const int cc[2] = {panel, n - next};
+    if (permute_cols(ctx, ws, A, lda, n, panel, pivots, panel_size, 0, nullptr, cb, cc, 2) !=
+        HDBF_STATUS_SUCCESS)
+        return;
+    offset_pivots_kernel<<<(panel_size + 255) / 256, 256, 0, stream>>>(pivots, panel_size, panel);
+}
+
+void launch_apply_getrf_permutation_double(double* A, int lda, int column_count,
+                                           const int* sources, const int* targets,
+                                           int move_count, double* temporary, int column_tile,
+                                           cudaStream_t stream)
+{
+    if (!A || column_count <= 0 || move_count <= 0 || column_tile <= 0) return;
+    hdbf_context* ctx = launcher_context(stream);
+    if (!ctx) return;
     int* cnt = ctx->dev_small + kSmallMoveCount + 1;
     cudaMemcpyAsync(cnt, &move_count, sizeof(int), cudaMemcpyHostToDevice, stream);
     apply_moves(ctx, A, lda, column_count, sources, targets, cnt, move_count, temporary,

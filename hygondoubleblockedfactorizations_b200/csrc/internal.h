@@ -141,12 +141,13 @@ void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st);
 //   coop  panel-kernel exchange slots (fixed size, offset 0)
 //   inv   inverted 64x64 diagonal blocks, ceil(n/64)*4096 floats
 //   perm  running composed row permutation of a GETRF outer block, n ints
+//   coop64  FP64 panel-kernel exchange slots (fixed size)
 //   src, tgt, gperm  composed row moves / permutation scratch, n ints each
 //   temp  column-tiled swap buffer, 64*n floats
 //   skinny  split-K partial sums of the skinny GEMM, 256*n floats
 //   wave  wavefront-solve row-major x copy (32 columns) and its flags
 struct WsLayout {
-    size_t coop, inv, perm, src, tgt, gperm, temp, skinny, wave, total;
+    size_t coop, inv, perm, coop64, src, tgt, gperm, temp, skinny, wave, total;
 };
 WsLayout ws_layout(int n);
 // Guarantee the layout for order n (grows the arena outside stream capture).
@@ -154,6 +155,7 @@ hdbf_status ensure_ws(hdbf_context* ctx, int n);
 float* ws_coop(hdbf_context* ctx);
 float* ws_inv(hdbf_context* ctx);
 int* ws_perm(hdbf_context* ctx);
+double* ws_coop64(hdbf_context* ctx);
 int* ws_src(hdbf_context* ctx);
 int* ws_tgt(hdbf_context* ctx);
 int* ws_gperm(hdbf_context* ctx);
@@ -330,6 +332,46 @@ struct GetrfWs {
 hdbf_status getrf_workspace(hdbf_context* ctx, int n, GetrfWs* ws);
 hdbf_status getrf_panel(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
                         int ipiv_add, int* info, int info_base, bool pivot, const GetrfWs& ws);
+
+// ---------------------------------------------------------------- FP64
+// Overloads of the primitives above for the `_double` entry points
+// (fp64.cu).  The FP64 workspace is the FP32 layout of order 2n.
+inline hdbf_status gemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
+                            const float* A, long long lda, const float* B, long long ldb,
+                            float* C, long long ldc)
+{
+    return sgemm_sub(ctx, nn, lower_only, M, N, K, A, lda, B, ldb, C, ldc);
+}
+hdbf_status gemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
+                     const double* A, long long lda, const double* B, long long ldb, double* C,
+                     long long ldc);
+hdbf_status gemm_sub_tn(hdbf_context* ctx, int M, int N, int K, const double* A, long long lda,
+                        const double* B, long long ldb, double* C, long long ldc);
+hdbf_status potf2_small(hdbf_context* ctx, int n, double* A, long long lda, int* info,
+                        int info_base);
+hdbf_status trsm_rlt(hdbf_context* ctx, int rows, int cols, const double* L, long long ldl,
+                     double* B, long long ldb);
+hdbf_status trsm_llu(hdbf_context* ctx, int rows, int cols, const double* L, long long ldl,
+                     double* B, long long ldb);
+hdbf_status syrk_lower(hdbf_context* ctx, int n, int k, const double* A, long long lda,
+                       double* C, long long ldc);
+hdbf_status potrf_diag(hdbf_context* ctx, int n, double* A, long long lda, int* info,
+                       int info_base);
+hdbf_status apply_moves(hdbf_context* ctx, double* A, long long lda, int ncols, const int* src,
+                        const int* tgt, const int* count, int max_moves, double* temp,
+                        long long temp_cols);
+hdbf_status getrf_panel(hdbf_context* ctx, int m, int w, double* A, long long lda, int* ipiv,
+                        int ipiv_add, int* info, int info_base, bool pivot, const GetrfWs& ws);
+size_t getf2_coop64_scratch_bytes();
+void configure_fp64_kernels(hdbf_context* ctx);
+// Workspace order for a problem of order n in scalar type T: FP64 needs the
+// FP32 layout of twice as many whole 64-row blocks (the inverse-block table
+// holds 4096 doubles per block).
+template <class T>
+inline int ws_order(int n) { return sizeof(T) == 8 ? 2 * ((n + 63) / 64 * 64) : n; }
+// Graph-cache key tag separating the FP32 and FP64 drivers.
+template <class T>
+inline long long type_tag() { return sizeof(T) == 8 ? 1000 : 0; }
 
 // ---------------------------------------------------------------- graphs
 // A whole factorization is a long chain of dependent launches; replaying it

@@ -90,6 +90,8 @@ WsLayout ws_layout(int n)
     off += align_up((size_t)(n + 63) / 64 * 64 * 64 * sizeof(float), 256);
     L.perm = off;
     off += align_up((size_t)n * sizeof(int), 256);
+    L.coop64 = off;
+    off += getf2_coop64_scratch_bytes();
     L.src = off;
     off += align_up((size_t)n * sizeof(int), 256);
     L.tgt = off;
@@ -134,6 +136,11 @@ float* ws_inv(hdbf_context* ctx)
 {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).inv);
 }
+double* ws_coop64(hdbf_context* ctx)
+{
+    return reinterpret_cast<double*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).coop64);
+}
+
 int* ws_perm(hdbf_context* ctx)
 {
     return reinterpret_cast<int*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).perm);
@@ -383,6 +390,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
     configure_trsm_block_kernels(ctx);
     configure_solve_kernels(ctx);
     configure_batched_kernels(ctx);
+    configure_fp64_kernels(ctx);
     const int one = 1;  // exchange epoch starts at 1: zeroed slots never match
     cudaMemcpy(ctx->dev_small + kSmallEpoch, &one, sizeof(int), cudaMemcpyHostToDevice);
     cudaDeviceSynchronize();

@@ -20,6 +20,15 @@ void gemm_nt_update_m_tiled(hdbf_handle handle, int rows, int cols, int k, const
                             int lda, const float* B, int ldb, float* C, int ldc,
                             int m_tile);
 
+/* reference update_gemm.h:20-29 (FP64 twin): C -= A * B^T */
+void gemm_nt_update_double(hdbf_handle handle, int rows, int cols, int k, const double* A,
+                           int lda, const double* B, int ldb, double* C, int ldc);
+
+/* reference update_gemm.h:43-52 (FP64 twin) */
+void gemm_nt_update_m_tiled_double(hdbf_handle handle, int rows, int cols, int k,
+                                   const double* A, int lda, const double* B, int ldb,
+                                   double* C, int ldc, int m_tile);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,10 @@ extern "C" {
 void blocked_right_looking_getrf(hdbf_handle handle, float* A, int lda, int n, int nb,
                                  int* ipiv, int* info);
 
+/* reference blocked_getrf.h:17-22 (FP64 twin) */
+void blocked_right_looking_getrf_double(hdbf_handle handle, double* A, int lda, int n, int nb,
+                                        int* ipiv, int* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,10 @@ extern "C" {
 void blocked_right_looking_getrf_npvt(hdbf_handle handle, float* A, int lda, int n,
                                       int nb, int* info);
 
+/* reference blocked_getrf_npvt.h:16-20 (FP64 twin) */
+void blocked_right_looking_getrf_npvt_double(hdbf_handle handle, double* A, int lda, int n,
+                                             int nb, int* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,20 @@ void double_blocked_getrf_batched_pivot(hdbf_handle handle, float* A, int lda, i
                                         int* info,
                                         getrf_batched_pivot_workspace* workspace);
 
+/* reference double_blocked_getrf.h:37-46 (FP64 twin, immediate pivots) */
+void double_blocked_getrf_double(hdbf_handle handle, double* A, int lda, int n, int outer_nb,
+                                 int inner_nb, getrf_outer_trsm_mode outer_trsm_mode,
+                                 int trsm_block, int* ipiv, int* info);
+
+/* reference double_blocked_getrf.h:62-74 (FP64 twin, batched pivots); the
+ * workspace's device_swap_buffer holds column_tile x n doubles. */
+void double_blocked_getrf_double_batched_pivot(hdbf_handle handle, double* A, int lda, int n,
+                                               int outer_nb, int inner_nb,
+                                               getrf_outer_trsm_mode outer_trsm_mode,
+                                               int trsm_block, int inner_gemm_m_tile, int* ipiv,
+                                               int* info,
+                                               getrf_batched_pivot_workspace* workspace);
+
 #ifdef __cplusplus
 }
 #endif

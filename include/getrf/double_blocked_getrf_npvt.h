@@ -13,6 +13,10 @@ extern "C" {
 void double_blocked_getrf_npvt(hdbf_handle handle, float* A, int lda, int n, int nb,
                                int b, int* info);
 
+/* reference double_blocked_getrf_npvt.h:17-23 (FP64 twin) */
+void double_blocked_getrf_npvt_double(hdbf_handle handle, double* A, int lda, int n, int nb,
+                                      int b, int* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,17 @@ void launch_apply_getrf_permutation(float* A, int lda, int column_count,
                                     float* temporary, int column_tile,
                                     cudaStream_t stream);
 
+/* reference getrf_pivot_kernels.h:17-23 (FP64 twin) */
+void launch_apply_getrf_panel_pivots_double(double* A, int lda, int n, int panel,
+                                            int panel_size, int* pivots, cudaStream_t stream);
+
+/* reference getrf_pivot_kernels.h:35-43 (FP64 twin); temporary holds
+ * column_tile x move_count doubles. */
+void launch_apply_getrf_permutation_double(double* A, int lda, int column_count,
+                                           const int* sources, const int* targets,
+                                           int move_count, double* temporary, int column_tile,
+                                           cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,26 @@ void double_blocked_potrf_kblocked_syrk_adaptive_gemm_configured(
     hdbf_handle handle, float* A, int lda, int n, int nb, int b, int syrk_k_tile,
     int gemm_m_tile, int gemm_m_threshold, int gemm_k_threshold, int* info);
 
+/* FP64 twins (reference double_blocked_potrf.h:57-103): same arguments and
+ * info convention, double-precision storage and arithmetic throughout. */
+/* reference double_blocked_potrf.h:57-63 */
+void double_blocked_potrf_double(hdbf_handle handle, double* A, int lda, int n, int nb, int b,
+                                 int* info);
+/* reference double_blocked_potrf.h:65-71 */
+void double_blocked_potrf_double_dbtrsm(hdbf_handle handle, double* A, int lda, int n, int nb,
+                                        int b, int* info);
+/* reference double_blocked_potrf.h:73-80 */
+void double_blocked_potrf_double_kblocked_syrk(hdbf_handle handle, double* A, int lda, int n,
+                                               int nb, int b, int syrk_k_tile, int* info);
+/* reference double_blocked_potrf.h:82-90 */
+void double_blocked_potrf_double_kblocked_syrk_adaptive_gemm(hdbf_handle handle, double* A,
+                                                             int lda, int n, int nb, int b,
+                                                             int syrk_k_tile, int* info);
+/* reference double_blocked_potrf.h:92-103 */
+void double_blocked_potrf_double_kblocked_syrk_adaptive_gemm_configured(
+    hdbf_handle handle, double* A, int lda, int n, int nb, int b, int syrk_k_tile,
+    int gemm_m_tile, int gemm_m_threshold, int gemm_k_threshold, int* info);
+
 #ifdef __cplusplus
 }
 #endif

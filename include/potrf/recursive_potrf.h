@@ -35,6 +35,11 @@ void recursive_potrf_tiled_trsm(hdbf_handle handle, StreamPool* pool, float* A, 
 void recursive_potrf_mixed_driver(hdbf_handle handle, StreamPool* pool, float* A, int lda,
                                   int n, int nb, int* info);
 
+/* reference recursive_potrf.h:24-29 (FP64 twin; the pool is accepted and,
+ * as in the FP32 entry point, the work runs on the handle's stream) */
+void recursive_potrf_double(hdbf_handle handle, StreamPool* pool, double* A, int lda, int n,
+                            int nb, int* info);
+
 #ifdef __cplusplus
 }
 #endif

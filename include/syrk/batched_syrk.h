@@ -20,6 +20,11 @@ void batched_syrk_bottom_up(hdbf_handle handle, StreamPool* pool, float* A, int 
 void batched_syrk_bottom_up_mixed(hdbf_handle handle, StreamPool* pool, float* A, int lda,
                                   float* C, int ldc, int n, int k, int nb);
 
+/* reference batched_syrk.h:32-35 (FP64 twin; the pool is accepted, the work
+ * runs on the handle's stream) */
+void batched_syrk_bottom_up_double(hdbf_handle handle, StreamPool* pool, double* A, int lda,
+                                   double* C, int ldc, int n, int k, int nb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,14 @@ void syrk_lower_update(hdbf_handle handle, int n, int k, const float* A, int lda
 void syrk_lower_update_kblocked(hdbf_handle handle, int n, int k, const float* A, int lda,
                                 float* C, int ldc, int k_tile);
 
+/* reference kblocked_syrk.h:17-23 (FP64 twin) */
+void syrk_lower_update_double(hdbf_handle handle, int n, int k, const double* A, int lda,
+                              double* C, int ldc);
+
+/* reference kblocked_syrk.h:34-41 (FP64 twin) */
+void syrk_lower_update_kblocked_double(hdbf_handle handle, int n, int k, const double* A,
+                                       int lda, double* C, int ldc, int k_tile);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,6 +14,10 @@ extern "C" {
 void recursive_syrk_parallel(hdbf_handle handle, float* A, int lda, float* C, int ldc,
                              int n, int k, int nb);
 
+/* reference recursive_syrk.h:25-30 (FP64 twin) */
+void recursive_syrk_parallel_double(hdbf_handle handle, double* A, int lda, double* C, int ldc,
+                                    int n, int k, int nb);
+
 #ifdef __cplusplus
 }
 #endif

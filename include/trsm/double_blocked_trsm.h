@@ -14,6 +14,10 @@ extern "C" {
 void double_blocked_trsm(hdbf_handle handle, float* A, int lda, float* B, int ldb, int n,
                          int m, int nb, int b);
 
+/* reference double_blocked_trsm.h:19-27 (FP64 twin) */
+void double_blocked_trsm_double(hdbf_handle handle, double* A, int lda, double* B, int ldb,
+                                int n, int m, int nb, int b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,10 @@ void recursive_trsm_tiled_update(hdbf_handle handle, float* A, int lda, float* B
 void recursive_trsm_mixed(hdbf_handle handle, float* A, int lda, float* B, int ldb, int n, int m,
                           int nb);
 
+/* reference recursive_trsm.h:29-33 (FP64 twin) */
+void recursive_trsm_double(hdbf_handle handle, double* A, int lda, double* B, int ldb, int n,
+                           int m, int nb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,10 @@ void trsm_right_lower_transpose(hdbf_handle handle, int rows, int cols, const fl
 hdbf_status trsm_right_lower_transpose_noalloc(int rows, int cols, const float* A, int lda,
                                                float* B, int ldb, cudaStream_t stream);
 
+/* reference right_lower_trsm.h:17-23 (FP64 twin): B <- B * L^{-T} */
+void trsm_right_lower_transpose_double(hdbf_handle handle, int rows, int cols, const double* A,
+                                       int lda, double* B, int ldb);
+
 #ifdef __cplusplus
 }
 #endif
