@@ -4,8 +4,9 @@
 // drivers in api_potrf.cu and api_getrf.cu are templates over the scalar
 // type; this file gives them the FP64 overloads of their primitives:
 //
-//   gemm_sub / gemm_sub_tn   C -= op(A) op(B), FP64 FMA, 64x64x16 tiles,
-//                            4x4 outputs per thread, lower-triangle mode
+//   gemm_sub / gemm_sub_tn   C -= op(A) op(B), FP64 FMA: 128x128x8 tiles with
+//                            8x8 outputs per thread for large updates, 64x64x16
+//                            with 4x4 for narrow ones; lower-triangle mode
 //   potf2_small              <= 64 Cholesky leaf, one CTA, LAPACK info
 //   tri_inv64                inverses of the 64x64 diagonal blocks
 //   trsm_rlt / trsm_llu      recursive TRSMs with inverse-apply leaves
@@ -42,24 +43,137 @@ inline int split64(int n)
 }
 
 // ------------------------------------------------------------------ GEMM
-constexpr int GBM = 64, GBN = 64, GBK = 16, GTHR = 256;
+// Large updates: 128x128x8 tiles, 256 threads, 8x8 outputs per thread in the split layout
+// (rows ty*4 + {0..3} and 64 + ty*4 + {0..3}, columns likewise with tx), so
+// every fragment is two 16-byte shared-memory loads; the next k-tile is
+// copied into the other shared-memory buffer with 8-byte cp.async (zero fill
+// outside the matrix) while the current one is consumed.
+constexpr int GBM = 128, GBN = 128, GBK = 8, GTHR = 256, GLD = GBM + 4;
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
 
 // MODE 0: C -= A B^T (A M x K, B N x K); 1: C -= A B (B K x N);
 // 2: C -= A^T B (A stored K x M, B K x N).  TRI: only entries with row >= col
 // (local to C) are written and tiles wholly above the diagonal are skipped.
 template <int MODE, bool TRI>
-__global__ void __launch_bounds__(GTHR) dgemm_sub_kernel(int M, int N, int K,
+__global__ void __launch_bounds__(GTHR, 1) dgemm_sub_kernel(int M, int N, int K,
+                                                            const double* __restrict__ A,
+                                                            long long lda,
+                                                            const double* __restrict__ B,
+                                                            long long ldb, double* C,
+                                                            long long ldc, int tiles_m)
+{
+    __shared__ __align__(16) double As[2][GBK][GLD];  // As[buf][k][m]
+    __shared__ __align__(16) double Bs[2][GBK][GLD];  // Bs[buf][k][n]
+    const int tile = blockIdx.x;
+    const int m0 = (tile % tiles_m) * GBM, n0 = (tile / tiles_m) * GBN;
+    if (TRI && n0 >= m0 + GBM) return;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    auto issue = [&](int buf, int k0) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int q = tid + e * GTHR;
+            int m, k;
+            if (MODE == 2) { k = q & 7; m = q >> 3; }
+            else { m = q & 127; k = q >> 7; }
+            const int gm = m0 + m, gk = k0 + k;
+            const bool va = gm < M && gk < K;
+            const double* pa =
+                va ? (MODE == 2 ? A + (long long)gm * lda + gk : A + (long long)gk * lda + gm) : A;
+            cp_async8(&As[buf][k][m], pa, va);
+            int nn, kk;
+            if (MODE == 0) { nn = q & 127; kk = q >> 7; }
+            else { kk = q & 7; nn = q >> 3; }
+            const int gn = n0 + nn, gk2 = k0 + kk;
+            const bool vb = gn < N && gk2 < K;
+            const double* pb =
+                vb ? (MODE == 0 ? B + (long long)gk2 * ldb + gn : B + (long long)gn * ldb + gk2)
+                   : B;
+            cp_async8(&Bs[buf][kk][nn], pb, vb);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int nk = (K + GBK - 1) / GBK;
+    issue(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int cur = kt & 1;
+        if (kt + 1 < nk) issue(cur ^ 1, (kt + 1) * GBK);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < GBK; ++k) {
+            double a[8], b[8];
+            const double2* ap = reinterpret_cast<const double2*>(&As[cur][k][ty * 4]);
+            const double2* ap2 = reinterpret_cast<const double2*>(&As[cur][k][64 + ty * 4]);
+            const double2* bp = reinterpret_cast<const double2*>(&Bs[cur][k][tx * 4]);
+            const double2* bp2 = reinterpret_cast<const double2*>(&Bs[cur][k][64 + tx * 4]);
+            const double2 a0 = ap[0], a1 = ap[1], a2 = ap2[0], a3 = ap2[1];
+            const double2 b0 = bp[0], b1 = bp[1], b2 = bp2[0], b3 = bp2[1];
+            a[0] = a0.x; a[1] = a0.y; a[2] = a1.x; a[3] = a1.y;
+            a[4] = a2.x; a[5] = a2.y; a[6] = a3.x; a[7] = a3.y;
+            b[0] = b0.x; b[1] = b0.y; b[2] = b1.x; b[3] = b1.y;
+            b[4] = b2.x; b[5] = b2.y; b[6] = b3.x; b[7] = b3.y;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int c = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+        if (c >= N) continue;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+            if (r < M && (!TRI || r >= c)) C[(long long)c * ldc + r] -= acc[i][j];
+        }
+    }
+}
+
+template <int MODE, bool TRI>
+void dgemm_launch(cudaStream_t s, int M, int N, int K, const double* A, long long lda,
+                  const double* B, long long ldb, double* C, long long ldc)
+{
+    const int tm = (M + GBM - 1) / GBM, tn = (N + GBN - 1) / GBN;
+    dgemm_sub_kernel<MODE, TRI><<<(unsigned)((long long)tm * tn), GTHR, 0, s>>>(
+        M, N, K, A, lda, B, ldb, C, ldc, tm);
+}
+
+// 64x64x16 tiles, 4x4 outputs per thread, register-staged prefetch: the
+// tall, narrow updates of the panels and TRSM recursions (more CTAs).
+constexpr int SBM = 64, SBN = 64, SBK = 16, STHR = 256;
+
+// MODE 0: C -= A B^T (A M x K, B N x K); 1: C -= A B (B K x N);
+// 2: C -= A^T B (A stored K x M, B K x N).  TRI: only entries with row >= col
+// (local to C) are written and tiles wholly above the diagonal are skipped.
+template <int MODE, bool TRI>
+__global__ void __launch_bounds__(STHR) dgemm_sub64_kernel(int M, int N, int K,
                                                          const double* __restrict__ A,
                                                          long long lda,
                                                          const double* __restrict__ B,
                                                          long long ldb, double* C, long long ldc,
                                                          int tiles_m)
 {
-    __shared__ double As[GBK][GBM + 1];
-    __shared__ double Bs[GBK][GBN + 1];
+    __shared__ double As[SBK][SBM + 1];
+    __shared__ double Bs[SBK][SBN + 1];
     const int tile = blockIdx.x;
-    const int m0 = (tile % tiles_m) * GBM, n0 = (tile / tiles_m) * GBN;
-    if (TRI && n0 >= m0 + GBM) return;
+    const int m0 = (tile % tiles_m) * SBM, n0 = (tile / tiles_m) * SBN;
+    if (TRI && n0 >= m0 + SBM) return;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     double acc[4][4];
 #pragma unroll
@@ -70,7 +184,7 @@ __global__ void __launch_bounds__(GTHR) dgemm_sub_kernel(int M, int N, int K,
     auto fetch = [&](int k0) {
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-            const int q = tid + e * GTHR;
+            const int q = tid + e * STHR;
             int m, k;
             if (MODE == 2) { k = q & 15; m = q >> 4; }
             else { m = q & 63; k = q >> 6; }
@@ -92,21 +206,21 @@ __global__ void __launch_bounds__(GTHR) dgemm_sub_kernel(int M, int N, int K,
     auto stash = [&]() {
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-            const int q = tid + e * GTHR;
+            const int q = tid + e * STHR;
             if (MODE == 2) As[q & 15][q >> 4] = ra[e];
             else As[q >> 6][q & 63] = ra[e];
             if (MODE == 0) Bs[q >> 6][q & 63] = rb[e];
             else Bs[q & 15][q >> 4] = rb[e];
         }
     };
-    const int nk = (K + GBK - 1) / GBK;
+    const int nk = (K + SBK - 1) / SBK;
     fetch(0);
     for (int kt = 0; kt < nk; ++kt) {
         stash();
         __syncthreads();
-        if (kt + 1 < nk) fetch((kt + 1) * GBK);
+        if (kt + 1 < nk) fetch((kt + 1) * SBK);
 #pragma unroll
-        for (int k = 0; k < GBK; ++k) {
+        for (int k = 0; k < SBK; ++k) {
             double a[4], b[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
@@ -132,11 +246,11 @@ __global__ void __launch_bounds__(GTHR) dgemm_sub_kernel(int M, int N, int K,
 }
 
 template <int MODE, bool TRI>
-void dgemm_launch(cudaStream_t s, int M, int N, int K, const double* A, long long lda,
+void dgemm_launch64(cudaStream_t s, int M, int N, int K, const double* A, long long lda,
                   const double* B, long long ldb, double* C, long long ldc)
 {
-    const int tm = (M + GBM - 1) / GBM, tn = (N + GBN - 1) / GBN;
-    dgemm_sub_kernel<MODE, TRI><<<(unsigned)((long long)tm * tn), GTHR, 0, s>>>(
+    const int tm = (M + SBM - 1) / SBM, tn = (N + SBN - 1) / SBN;
+    dgemm_sub64_kernel<MODE, TRI><<<(unsigned)((long long)tm * tn), STHR, 0, s>>>(
         M, N, K, A, lda, B, ldb, C, ldc, tm);
 }
 
@@ -147,7 +261,7 @@ hdbf_status dgemm(hdbf_context* ctx, int mode, bool lower_only, int M, int N, in
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
     if (!A || !B || !C) return HDBF_STATUS_INVALID_VALUE;
     if (lower_only && mode != 0) return HDBF_STATUS_INVALID_VALUE;
-    const long long tiles = (long long)((M + GBM - 1) / GBM) * ((N + GBN - 1) / GBN);
+    const long long tiles = (long long)((M + SBM - 1) / SBM) * ((N + SBN - 1) / SBN);
     if (tiles > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
     double flops = 2.0 * (double)M * N * K;
     if (lower_only) {
@@ -157,13 +271,26 @@ hdbf_status dgemm(hdbf_context* ctx, int mode, bool lower_only, int M, int N, in
     ProfScope prof(ctx, kClsGemm, flops, 8.0 * ((double)M * K + (double)N * K + 2.0 * M * N), M,
                    N, K);
     cudaStream_t s = ctx->stream;
-    if (mode == 0) {
-        if (lower_only) dgemm_launch<0, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
-        else dgemm_launch<0, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
-    } else if (mode == 1) {
-        dgemm_launch<1, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+    // 128x128 tiles only when they still give two waves of CTAs (one per SM)
+    const long long big_tiles = (long long)((M + GBM - 1) / GBM) * ((N + GBN - 1) / GBN);
+    if (big_tiles >= 2LL * ctx->sm_count) {
+        if (mode == 0) {
+            if (lower_only) dgemm_launch<0, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
+            else dgemm_launch<0, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        } else if (mode == 1) {
+            dgemm_launch<1, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        } else {
+            dgemm_launch<2, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        }
     } else {
-        dgemm_launch<2, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        if (mode == 0) {
+            if (lower_only) dgemm_launch64<0, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
+            else dgemm_launch64<0, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        } else if (mode == 1) {
+            dgemm_launch64<1, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        } else {
+            dgemm_launch64<2, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        }
     }
     ctx->launches++;
     return last_cuda(ctx);
