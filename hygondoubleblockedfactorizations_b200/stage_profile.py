@@ -16,7 +16,9 @@ launches, milliseconds, share of the device time and TFLOP/s or GB/s.
 ``double_blocked_getrf_batched_pivot`` (iterative outer TRSM, as the
 benchmark does) instead of ``double_blocked_getrf``, and ``--lookahead 0|1``
 sets the handle's GETRF look-ahead.  Mixed precisions use ``hdbf_spotrf_mixed`` / ``hdbf_sgetrf_mixed``
-with panel width ``--inner``.
+with panel width ``--inner``; ``--precision fp64`` runs the FP64 twins
+``double_blocked_potrf_double`` / ``double_blocked_getrf_double`` (iterative
+outer TRSM) on the same inputs widened to FP64.
 """
 from __future__ import annotations
 
@@ -33,7 +35,7 @@ def main(argv=None):
 
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--op", choices=["potrf", "getrf"], default="getrf")
-    ap.add_argument("--precision", choices=list(PREC), default="fp32")
+    ap.add_argument("--precision", choices=list(PREC) + ["fp64"], default="fp32")
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--outer", type=int, default=8192)
     ap.add_argument("--inner", type=int, default=512)
@@ -52,6 +54,8 @@ def main(argv=None):
         h.set_lookahead(bool(a.lookahead))
     n = a.n
     A0 = _matrix(torch, h, a.op, n, a.seed)
+    if a.precision == "fp64":
+        A0 = A0.double()
     A = torch.empty_like(A0)
     ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -69,7 +73,13 @@ def main(argv=None):
 
     def run():
         A.copy_(A0)
-        if a.precision == "fp32" and a.op == "potrf":
+        if a.precision == "fp64" and a.op == "potrf":
+            call("double_blocked_potrf_double", h.ptr, P(A.data_ptr()), n, n, a.outer, a.inner,
+                 P(info.data_ptr()))
+        elif a.precision == "fp64":
+            call("double_blocked_getrf_double", h.ptr, P(A.data_ptr()), n, n, a.outer, a.inner,
+                 1, 0, P(ipiv.data_ptr()), P(info.data_ptr()))
+        elif a.precision == "fp32" and a.op == "potrf":
             call("double_blocked_potrf_kblocked_syrk", h.ptr, P(A.data_ptr()), n, n, a.outer,
                  a.inner, 0, P(info.data_ptr()))
         elif a.precision == "fp32" and a.batched:
