@@ -63,6 +63,10 @@ def lib():
         L.oracle_double_blocked_potrf.argtypes = [dp, i, i, i, i, i]
         L.oracle_double_blocked_getrf.restype = i
         L.oracle_double_blocked_getrf.argtypes = [dp, i, i, i, i, dp]
+        L.oracle_double_blocked_potrf_f64.restype = i
+        L.oracle_double_blocked_potrf_f64.argtypes = [dp, i, i, i, i, i]
+        L.oracle_double_blocked_getrf_f64.restype = i
+        L.oracle_double_blocked_getrf_f64.argtypes = [dp, i, i, i, i, dp]
         L.oracle_parse_seed.restype = i
         L.oracle_parse_seed.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint)]
         _lib = L
@@ -189,7 +193,7 @@ def getrf_residual_blas(LU2d: np.ndarray, A2d: np.ndarray, ipiv) -> float:
     return _ratio(_ssq_norm(L @ U - PA), _ssq_norm(PA))
 
 
-# --- reference loops restated in C (FP32) ----------------------------------
+# --- reference loops restated in C (FP32 and FP64) -------------------------
 
 def double_blocked_potrf(A2d: np.ndarray, nb: int, b: int, syrk_k_tile: int = 0):
     A = np.asfortranarray(np.array(A2d, dtype=np.float32))
@@ -197,6 +201,26 @@ def double_blocked_potrf(A2d: np.ndarray, nb: int, b: int, syrk_k_tile: int = 0)
     info = lib().oracle_double_blocked_potrf(A.ctypes.data_as(ctypes.c_void_p), n, n,
                                              nb, b, syrk_k_tile)
     return A, info
+
+
+def double_blocked_potrf_f64(A2d: np.ndarray, nb: int, b: int, syrk_k_tile: int = 0):
+    """FP64 twin of double_blocked_potrf (the same loops in double)."""
+    A = np.asfortranarray(np.array(A2d, dtype=np.float64))
+    n = A.shape[0]
+    info = lib().oracle_double_blocked_potrf_f64(A.ctypes.data_as(ctypes.c_void_p), n, n,
+                                                 nb, b, syrk_k_tile)
+    return A, info
+
+
+def double_blocked_getrf_f64(A2d: np.ndarray, outer_nb: int, inner_nb: int):
+    """FP64 twin of double_blocked_getrf (the same loops in double)."""
+    A = np.asfortranarray(np.array(A2d, dtype=np.float64))
+    n = A.shape[0]
+    ipiv = np.zeros(n, dtype=np.int32)
+    info = lib().oracle_double_blocked_getrf_f64(A.ctypes.data_as(ctypes.c_void_p), n, n,
+                                                 outer_nb, inner_nb,
+                                                 ipiv.ctypes.data_as(ctypes.c_void_p))
+    return A, ipiv, info
 
 
 def double_blocked_getrf(A2d: np.ndarray, outer_nb: int, inner_nb: int):

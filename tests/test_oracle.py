@@ -186,3 +186,32 @@ def test_generator_values():
     A = oracle.spd_gram(64, 0)
     np.testing.assert_array_equal(A, A.T)
     assert np.linalg.eigvalsh(A.astype(np.float64)).min() > 0.9
+
+
+@pytest.mark.parametrize("n,nb,b", [(200, 64, 16), (300, 128, 32), (97, 40, 7), (1, 8, 4)])
+def test_c_double_blocked_loops_f64_match_lapack(n, nb, b):
+    """The FP64 twins of the restated loops reproduce host LAPACK dpotrf /
+    dgetrf: factors to FP64 rounding, identical pivots, info on failure."""
+    from scipy.linalg import lapack
+    G = oracle.general_uniform(n, 0).astype(np.float64)
+    A = G @ G.T / n + np.eye(n)
+    A = 0.5 * (A + A.T)
+    L, info = oracle.double_blocked_potrf_f64(A, nb, b, syrk_k_tile=nb // 2)
+    ref, rinfo = lapack.dpotrf(np.asfortranarray(A), lower=1, clean=1)
+    assert info == rinfo == 0
+    assert np.abs(np.tril(L) - ref).max() <= 1e-13 * np.abs(ref).max()
+    M = oracle.general_uniform(n, 1).astype(np.float64)
+    LU, ipiv, info = oracle.double_blocked_getrf_f64(M, nb, b)
+    lu_l, ipiv_l, info_l = oracle.lapack_dgetrf(M)
+    assert info == info_l == 0
+    np.testing.assert_array_equal(ipiv, ipiv_l)
+    assert np.abs(LU - lu_l).max() <= 1e-12 * np.abs(lu_l).max()
+    # a failing column: same info as LAPACK
+    if n > 50:
+        A[50, 50] = -1.0
+        _, info = oracle.double_blocked_potrf_f64(A, nb, b)
+        _, rinfo = lapack.dpotrf(np.asfortranarray(A), lower=1)
+        assert info == rinfo == 51
+        M[:, 30] = 0.0
+        _, _, info = oracle.double_blocked_getrf_f64(M, nb, b)
+        assert info == oracle.lapack_dgetrf(M)[2] == 31
