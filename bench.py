@@ -490,7 +490,7 @@ def gpu_index():
 DEFAULTS = dict(potrf_nb=4096, potrf_b=512, potrf_tk=0, getrf_nb=8192, getrf_b=1024,
                 getrf_trsm_block=0, getrf_mtile=0, getrf_pivot_tile=64)
 
-# The reference's published K100 AI numbers at n = 32768:
+# The reference's published K100 AI numbers at n = 32768 (its paper-final scaling runs):
 # POTRF DoubleBlock+KBSYRK 565.6 ms, GETRF DB-LU+BatchedPivot+MGEMM 2152.1 ms.
 REF_PUBLISHED_MS = {"potrf": 565.6, "getrf": 2152.1}
 
