@@ -67,6 +67,11 @@ def lib():
         L.oracle_double_blocked_potrf_f64.argtypes = [dp, i, i, i, i, i]
         L.oracle_double_blocked_getrf_f64.restype = i
         L.oracle_double_blocked_getrf_f64.argtypes = [dp, i, i, i, i, dp]
+        for name in ("oracle_double_blocked_getrf_batched_f32",
+                     "oracle_double_blocked_getrf_batched_f64"):
+            f = getattr(L, name)
+            f.restype = i
+            f.argtypes = [dp, i, i, i, i, dp]
         L.oracle_parse_seed.restype = i
         L.oracle_parse_seed.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint)]
         _lib = L
@@ -220,6 +225,19 @@ def double_blocked_getrf_f64(A2d: np.ndarray, outer_nb: int, inner_nb: int):
     info = lib().oracle_double_blocked_getrf_f64(A.ctypes.data_as(ctypes.c_void_p), n, n,
                                                  outer_nb, inner_nb,
                                                  ipiv.ctypes.data_as(ctypes.c_void_p))
+    return A, ipiv, info
+
+
+def double_blocked_getrf_batched(A2d: np.ndarray, outer_nb: int, inner_nb: int,
+                                 dtype=np.float32):
+    """Batched-pivot schedule of the double-blocked LU (FP32 or FP64)."""
+    A = np.asfortranarray(np.array(A2d, dtype=dtype))
+    n = A.shape[0]
+    ipiv = np.zeros(n, dtype=np.int32)
+    fn = (lib().oracle_double_blocked_getrf_batched_f64 if A.dtype == np.float64
+          else lib().oracle_double_blocked_getrf_batched_f32)
+    info = fn(A.ctypes.data_as(ctypes.c_void_p), n, n, outer_nb, inner_nb,
+              ipiv.ctypes.data_as(ctypes.c_void_p))
     return A, ipiv, info
 
 

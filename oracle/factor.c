@@ -12,6 +12,8 @@
  *       update_next_inner_panel  src/potrf/double_blocked_potrf.cpp:210-249
  *       prepare_next_outer_panel src/potrf/double_blocked_potrf.cpp:251-292
  *   oracle_double_blocked_getrf  src/getrf/double_blocked_getrf.cpp:125-191
+ *   oracle_double_blocked_getrf_batched
+ *                                src/getrf/getrf_batched_pivot_internal.h:445-624
  *       prepare_next_inner_panel src/getrf/double_blocked_getrf.cpp:32-71
  *       prepare_next_outer_panel src/getrf/double_blocked_getrf.cpp:73-123
  *       apply_panel_pivots       src/getrf/getrf_pivot_kernels.hip:14-45

@@ -233,3 +233,70 @@ int F(oracle_double_blocked_getrf)(REAL* A, int lda, int n, int outer_nb,
     }
     return info;
 }
+
+/* Rows r = k0..k1-1 of the LAPACK swap list ipiv (1-based GLOBAL rows) applied
+ * in order to columns [c0, c0 + nc). */
+static void F(swap_rows)(REAL* A, int lda, const int* ipiv, int k0, int k1, int c0, int nc)
+{
+    for (int c = c0; c < c0 + nc; ++c)
+        for (int r = k0; r < k1; ++r) {
+            int p = ipiv[r] - 1;
+            if (p != r) {
+                REAL t = AT(A, lda, r, c);
+                AT(A, lda, r, c) = AT(A, lda, p, c);
+                AT(A, lda, p, c) = t;
+            }
+        }
+}
+
+/*
+ * Double-blocked left-looking LU with batched pivots
+ * (src/getrf/getrf_batched_pivot_internal.h:445-624), outer TRSM direct:
+ * after each panel its interchanges reach only the block's columns
+ * ("inner pivot batch", :483-516); at the end of an outer block the block's
+ * interchanges reach the earlier columns and every interchange so far reaches
+ * the next block's columns ("outer pivot batch", :556-609), before that
+ * block's outer TRSM + GEMM.  The host composition of the swaps into moved
+ * rows (:59-223) is the same data movement as applying the swaps in order.
+ * ipiv receives 1-based GLOBAL rows; the factors equal the immediate-pivot
+ * loop's bit for bit.
+ */
+int F(oracle_double_blocked_getrf_batched)(REAL* A, int lda, int n, int outer_nb,
+                                            int inner_nb, int* ipiv)
+{
+    int info = 0;
+    if (n <= 0) return 0;
+    if (outer_nb <= 0) outer_nb = n;
+    if (inner_nb <= 0) inner_nb = outer_nb;
+    inner_nb = imin(inner_nb, outer_nb);
+    for (int outer = 0; outer < n; outer += outer_nb) {
+        int outer_end = outer + imin(outer_nb, n - outer);
+        for (int inner = outer; inner < outer_end; inner += inner_nb) {
+            int isz = imin(inner_nb, outer_end - inner);
+            int next = inner + isz;
+            int f = F(getf2)(n - inner, isz, &AT(A, lda, inner, inner), lda, ipiv + inner);
+            if (f && !info) info = inner + f;
+            for (int o = 0; o < isz; ++o) ipiv[inner + o] += inner;
+            F(swap_rows)(A, lda, ipiv, inner, next, outer, inner - outer);
+            F(swap_rows)(A, lda, ipiv, inner, next, next, outer_end - next);
+            if (next < outer_end) {
+                int nsz = imin(inner_nb, outer_end - next);
+                int hist = next - outer;
+                F(trsm_left_lower_unit)(hist, nsz, &AT(A, lda, outer, outer), lda,
+                                        &AT(A, lda, outer, next), lda);
+                F(gemm_nn_sub)(n - next, nsz, hist, &AT(A, lda, next, outer), lda,
+                               &AT(A, lda, outer, next), lda, &AT(A, lda, next, next), lda);
+            }
+        }
+        if (outer > 0) F(swap_rows)(A, lda, ipiv, outer, outer_end, 0, outer);
+        if (outer_end < n) {
+            int next = outer_end;
+            int nsz = imin(outer_nb, n - next);
+            F(swap_rows)(A, lda, ipiv, 0, outer_end, next, nsz);
+            F(trsm_left_lower_unit)(next, nsz, A, lda, &AT(A, lda, 0, next), lda);
+            F(gemm_nn_sub)(n - next, nsz, next, &AT(A, lda, next, 0), lda,
+                           &AT(A, lda, 0, next), lda, &AT(A, lda, next, next), lda);
+        }
+    }
+    return info;
+}

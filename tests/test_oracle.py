@@ -215,3 +215,25 @@ def test_c_double_blocked_loops_f64_match_lapack(n, nb, b):
         M[:, 30] = 0.0
         _, _, info = oracle.double_blocked_getrf_f64(M, nb, b)
         assert info == oracle.lapack_dgetrf(M)[2] == 31
+
+
+@pytest.mark.parametrize("n,nb,b", [(200, 64, 16), (300, 128, 32), (97, 40, 7), (256, 256, 64),
+                                    (1, 8, 4)])
+def test_batched_pivot_schedule_equals_immediate(n, nb, b):
+    """The batched-pivot schedule (interchanges deferred to the block's columns,
+    then to earlier and next-block columns at the end of each outer block)
+    moves the same data as applying every panel's swaps at once: factors and
+    pivots are bit-identical to the immediate-pivot loop in FP32 and FP64,
+    and the pivots are host LAPACK's."""
+    G = oracle.general_uniform(n, 1)
+    LU_i, ipiv_i, info_i = oracle.double_blocked_getrf(G, nb, b)
+    LU_b, ipiv_b, info_b = oracle.double_blocked_getrf_batched(G, nb, b)
+    np.testing.assert_array_equal(LU_b, LU_i)
+    np.testing.assert_array_equal(ipiv_b, ipiv_i)
+    assert info_b == info_i == 0
+    np.testing.assert_array_equal(ipiv_b, oracle.lapack_sgetrf(G)[1])
+    G64 = G.astype(np.float64)
+    LU_i, ipiv_i, _ = oracle.double_blocked_getrf_f64(G64, nb, b)
+    LU_b, ipiv_b, _ = oracle.double_blocked_getrf_batched(G64, nb, b, dtype=np.float64)
+    np.testing.assert_array_equal(LU_b, LU_i)
+    np.testing.assert_array_equal(ipiv_b, oracle.lapack_dgetrf(G64)[1])
