@@ -300,3 +300,85 @@ int F(oracle_double_blocked_getrf_batched)(REAL* A, int lda, int n, int outer_nb
     }
     return info;
 }
+
+/* LAPACK xGETF2 without row interchanges (the NPVT panels): returns 0 or the
+ * 1-based local column of the first exact zero pivot. */
+static int F(getf2_npvt)(int m, int w, REAL* A, int lda)
+{
+    int info = 0;
+    const REAL sfmin = SFMIN;
+    for (int j = 0; j < imin(m, w); ++j) {
+        REAL piv = AT(A, lda, j, j);
+        if (piv != 0.0f) {
+            if (FABS(piv) >= sfmin) {
+                REAL r = 1.0f / piv;
+                for (int i = j + 1; i < m; ++i) AT(A, lda, i, j) *= r;
+            } else {
+                for (int i = j + 1; i < m; ++i) AT(A, lda, i, j) /= piv;
+            }
+        } else if (!info) {
+            info = j + 1;
+        }
+        for (int k = j + 1; k < w; ++k) {
+            REAL u = AT(A, lda, j, k);
+            for (int i = j + 1; i < m; ++i) AT(A, lda, i, k) -= AT(A, lda, i, j) * u;
+        }
+    }
+    return info;
+}
+
+/*
+ * Blocked right-looking Cholesky, lower (src/potrf/blocked_potrf.cpp:127-181):
+ * per block column potf2 on the diagonal block, the panel TRSM and the lower
+ * SYRK of the whole trailing matrix.
+ */
+int F(oracle_blocked_right_looking_potrf)(REAL* A, int lda, int n, int nb)
+{
+    int info = 0;
+    if (n <= 0) return 0;
+    if (nb <= 0) nb = n;
+    for (int k = 0; k < n; k += nb) {
+        int psz = imin(nb, n - k);
+        int tr = n - k - psz;
+        int f = F(potf2_lower)(psz, &AT(A, lda, k, k), lda);
+        if (f && !info) info = k + f;
+        if (tr <= 0) continue;
+        F(trsm_right_lower_trans)(tr, psz, &AT(A, lda, k, k), lda, &AT(A, lda, k + psz, k), lda);
+        F(syrk_lower_sub)(tr, psz, &AT(A, lda, k + psz, k), lda, &AT(A, lda, k + psz, k + psz),
+                          lda);
+    }
+    return info;
+}
+
+/*
+ * Blocked right-looking LU (src/getrf/blocked_getrf.cpp:15-71; pivot = 0 gives
+ * the NPVT variant, src/getrf/blocked_getrf_npvt.cpp): panel GETF2 over the
+ * remaining rows, its interchanges on every other column, the U12 TRSM and
+ * the trailing GEMM.  ipiv (1-based GLOBAL rows) is written when pivoting.
+ */
+int F(oracle_blocked_right_looking_getrf)(REAL* A, int lda, int n, int nb, int* ipiv,
+                                          int pivot)
+{
+    int info = 0;
+    if (n <= 0) return 0;
+    if (nb <= 0) nb = n;
+    for (int p = 0; p < n; p += nb) {
+        int psz = imin(nb, n - p);
+        int next = p + psz;
+        int tr = n - next;
+        int f;
+        if (pivot) {
+            f = F(getf2)(n - p, psz, &AT(A, lda, p, p), lda, ipiv + p);
+            F(apply_panel_pivots)(A, lda, n, p, psz, ipiv + p);
+            for (int o = 0; o < psz; ++o) ipiv[p + o] += p;
+        } else {
+            f = F(getf2_npvt)(n - p, psz, &AT(A, lda, p, p), lda);
+        }
+        if (f && !info) info = p + f;
+        if (tr <= 0) continue;
+        F(trsm_left_lower_unit)(psz, tr, &AT(A, lda, p, p), lda, &AT(A, lda, p, next), lda);
+        F(gemm_nn_sub)(tr, tr, psz, &AT(A, lda, next, p), lda, &AT(A, lda, p, next), lda,
+                       &AT(A, lda, next, next), lda);
+    }
+    return info;
+}

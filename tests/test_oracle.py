@@ -237,3 +237,36 @@ def test_batched_pivot_schedule_equals_immediate(n, nb, b):
     LU_b, ipiv_b, _ = oracle.double_blocked_getrf_batched(G64, nb, b, dtype=np.float64)
     np.testing.assert_array_equal(LU_b, LU_i)
     np.testing.assert_array_equal(ipiv_b, oracle.lapack_dgetrf(G64)[1])
+
+
+@pytest.mark.parametrize("n,nb", [(200, 48), (97, 32), (1, 4), (130, 130)])
+def test_right_looking_baselines_match_lapack(n, nb):
+    """The right-looking POTRF / GETRF baselines and the NPVT variant restated
+    in C: Cholesky factors and info as host LAPACK (FP32 within the scaled
+    residual bound, FP64 to rounding), LU pivots identical to sgetrf/dgetrf,
+    NPVT equal to LAPACK's LU when diagonal dominance makes the pivots the
+    identity."""
+    from scipy.linalg import lapack
+    A = oracle.spd_gram(n, 0)
+    L, info = oracle.blocked_right_looking_potrf(A, nb)
+    assert info == 0 and oracle.scaled(oracle.potrf_residual_blas(L, A), n) <= 10
+    A64 = A.astype(np.float64)
+    L64, info = oracle.blocked_right_looking_potrf(A64, nb, dtype=np.float64)
+    ref, rinfo = lapack.dpotrf(np.asfortranarray(A64), lower=1, clean=1)
+    assert info == rinfo == 0
+    assert np.abs(np.tril(L64) - ref).max() <= 1e-13 * np.abs(ref).max()
+    G = oracle.general_uniform(n, 1)
+    LU, ipiv, info = oracle.blocked_right_looking_getrf(G, nb)
+    assert info == 0
+    np.testing.assert_array_equal(ipiv, oracle.lapack_sgetrf(G)[1])
+    assert oracle.scaled(oracle.getrf_residual_blas(LU, G, ipiv), n) <= 10
+    G64 = G.astype(np.float64)
+    LU64, ipiv64, _ = oracle.blocked_right_looking_getrf(G64, nb, dtype=np.float64)
+    lu_l, ipiv_l, _ = oracle.lapack_dgetrf(G64)
+    np.testing.assert_array_equal(ipiv64, ipiv_l)
+    assert np.abs(LU64 - lu_l).max() <= 1e-12 * np.abs(lu_l).max()
+    D = G64 + n * np.eye(n)
+    LUn, _, info = oracle.blocked_right_looking_getrf(D, nb, pivot=False, dtype=np.float64)
+    lu_d, piv_d, _ = oracle.lapack_dgetrf(D)
+    assert info == 0 and np.array_equal(piv_d, np.arange(1, n + 1))
+    assert np.abs(LUn - lu_d).max() <= 1e-13 * np.abs(lu_d).max()
