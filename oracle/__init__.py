@@ -68,6 +68,9 @@ def lib():
         L.oracle_double_blocked_getrf_f64.restype = i
         L.oracle_double_blocked_getrf_f64.argtypes = [dp, i, i, i, i, dp]
         for sfx in ("f32", "f64"):
+            f = getattr(L, "oracle_recursive_potrf_" + sfx)
+            f.restype = i
+            f.argtypes = [dp, i, i, i]
             f = getattr(L, "oracle_blocked_right_looking_potrf_" + sfx)
             f.restype = i
             f.argtypes = [dp, i, i, i]
@@ -246,6 +249,16 @@ def double_blocked_getrf_batched(A2d: np.ndarray, outer_nb: int, inner_nb: int,
     info = fn(A.ctypes.data_as(ctypes.c_void_p), n, n, outer_nb, inner_nb,
               ipiv.ctypes.data_as(ctypes.c_void_p))
     return A, ipiv, info
+
+
+def recursive_potrf(A2d: np.ndarray, nb: int, dtype=np.float32):
+    """Recursive Cholesky (FP32 or FP64)."""
+    A = np.asfortranarray(np.array(A2d, dtype=dtype))
+    n = A.shape[0]
+    sfx = "f64" if A.dtype == np.float64 else "f32"
+    info = getattr(lib(), "oracle_recursive_potrf_" + sfx)(
+        A.ctypes.data_as(ctypes.c_void_p), n, n, nb)
+    return A, info
 
 
 def blocked_right_looking_potrf(A2d: np.ndarray, nb: int, dtype=np.float32):

@@ -14,6 +14,7 @@
  *   oracle_double_blocked_getrf  src/getrf/double_blocked_getrf.cpp:125-191
  *   oracle_double_blocked_getrf_batched
  *                                src/getrf/getrf_batched_pivot_internal.h:445-624
+ *   oracle_recursive_potrf       src/potrf/recursive_potrf.cpp:17-174
  *   oracle_blocked_right_looking_potrf  src/potrf/blocked_potrf.cpp:127-181
  *   oracle_blocked_right_looking_getrf  src/getrf/blocked_getrf.cpp:15-71
  *                                       (pivot = 0: blocked_getrf_npvt.cpp)

@@ -382,3 +382,28 @@ int F(oracle_blocked_right_looking_getrf)(REAL* A, int lda, int n, int nb, int* 
     }
     return info;
 }
+
+/*
+ * Recursive Cholesky, lower (src/potrf/recursive_potrf.cpp:17-174): below
+ * order nb the diagonal POTRF; above it the split n1 = n/2, POTRF(A11),
+ * A21 <- A21 L11^{-T}, A22 -= A21 A21^T, POTRF(A22).  info is global.
+ */
+static int F(rec_potrf)(REAL* A, int lda, int n, int nb, int base)
+{
+    if (n <= 0) return 0;
+    if (nb <= 0 || n <= nb) {
+        int f = F(potf2_lower)(n, A, lda);
+        return f ? base + f : 0;
+    }
+    int n1 = n / 2, n2 = n - n1;
+    int info = F(rec_potrf)(A, lda, n1, nb, base);
+    if (info) return info;
+    F(trsm_right_lower_trans)(n2, n1, A, lda, &AT(A, lda, n1, 0), lda);
+    F(syrk_lower_sub)(n2, n1, &AT(A, lda, n1, 0), lda, &AT(A, lda, n1, n1), lda);
+    return F(rec_potrf)(&AT(A, lda, n1, n1), lda, n2, nb, base + n1);
+}
+
+int F(oracle_recursive_potrf)(REAL* A, int lda, int n, int nb)
+{
+    return F(rec_potrf)(A, lda, n, nb, 0);
+}

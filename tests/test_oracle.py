@@ -270,3 +270,23 @@ def test_right_looking_baselines_match_lapack(n, nb):
     lu_d, piv_d, _ = oracle.lapack_dgetrf(D)
     assert info == 0 and np.array_equal(piv_d, np.arange(1, n + 1))
     assert np.abs(LUn - lu_d).max() <= 1e-13 * np.abs(lu_d).max()
+
+
+@pytest.mark.parametrize("n,nb", [(200, 48), (97, 32), (1, 4), (300, 64)])
+def test_recursive_potrf_matches_lapack(n, nb):
+    """The recursive Cholesky restated in C: factors as host LAPACK (FP32
+    within the scaled residual bound, FP64 to rounding) and LAPACK's info for
+    a matrix with a failing column."""
+    from scipy.linalg import lapack
+    A = oracle.spd_gram(n, 5)
+    L, info = oracle.recursive_potrf(A, nb)
+    assert info == 0 and oracle.scaled(oracle.potrf_residual_blas(L, A), n) <= 10
+    A64 = A.astype(np.float64)
+    L64, info = oracle.recursive_potrf(A64, nb, dtype=np.float64)
+    ref, rinfo = lapack.dpotrf(np.asfortranarray(A64), lower=1, clean=1)
+    assert info == rinfo == 0
+    assert np.abs(np.tril(L64) - ref).max() <= 1e-13 * np.abs(ref).max()
+    if n > 80:
+        A64[80, 80] = -1.0
+        _, info = oracle.recursive_potrf(A64, nb, dtype=np.float64)
+        assert info == lapack.dpotrf(np.asfortranarray(A64), lower=1)[1] == 81
