@@ -12,6 +12,11 @@ Contents
   FP64 product done by host BLAS (numpy), the analogue of the reference's
   ``HYGON_CPU_FP64_USE_CBLAS`` mode (``cpu_fp64_residual.h:52-71``); pinned
   against the C version on small sizes by the tests.
+* ``potrf_residual_tiled`` / ``getrf_residual_tiled`` -- the same quantity block
+  column by block column (host BLAS, a few FP64 blocks resident), for the
+  orders 8192 ... 49152 of the sweep; pinned against the C version too.
+* ``pivot_divergence`` -- first index where two pivot sequences differ and the
+  FP64 relative gap of the two candidates there (near-tie test).
 * ``double_blocked_potrf`` / ``double_blocked_getrf`` -- plain-C FP32 restatement
   of the reference loops (``factor.c``).
 * ``lapack_spotrf`` / ``lapack_sgetrf`` -- host LAPACK (SciPy's OpenBLAS), the
@@ -35,11 +40,18 @@ EPS64 = float(np.finfo(np.float64).eps)
 _lib = None
 
 
+def reference_root() -> str:
+    """The reference checkout the oracle's _ref build reads (read-only):
+    $HDBF_REFERENCE_ROOT, else /root/reference."""
+    return os.environ.get("HDBF_REFERENCE_ROOT", "/root/reference")
+
+
 def build() -> str:
     """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    if os.path.isdir("/root/reference/include"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    ref = reference_root()
+    if os.path.isdir(os.path.join(ref, "include")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={ref}"], check=True)
     return os.path.join(_HERE, "liboracle.so")
 
 
@@ -208,6 +220,116 @@ def getrf_residual_blas(LU2d: np.ndarray, A2d: np.ndarray, ipiv) -> float:
     return _ratio(_ssq_norm(L @ U - PA), _ssq_norm(PA))
 
 
+# --- tiled BLAS residuals for large orders ---------------------------------
+#
+# The same quantities as potrf_residual / getrf_residual
+# (cpu_fp64_residual.h:73-201: FP32 values widened to FP64 before they are
+# multiplied, structurally zero triangular products skipped, Frobenius norms
+# of the whole residual and of the whole original), computed block column by
+# block column with host BLAS so that orders of 32768 and 49152 finish in
+# seconds to minutes on the host's cores and hold only a few column blocks in
+# FP64 at a time.  The norms merge per-block (scale, sum of squares) pairs as
+# the reference's overflow-safe accumulation does (cpu_fp64_residual.h:29-50).
+
+class _Ssq:
+    def __init__(self):
+        self.scale, self.sumsq, self.finite = 0.0, 1.0, True
+
+    def add(self, x: np.ndarray):
+        if x.size == 0:
+            return
+        hi, lo = float(np.max(x)), float(np.min(x))
+        m = max(abs(hi), abs(lo))
+        if not np.isfinite(m) or np.isnan(hi) or np.isnan(lo):
+            self.finite = False
+            return
+        if m == 0.0:
+            return
+        if 1e-150 < m < 1e150:  # no overflow or underflow of x*x: plain dot
+            flat = np.ascontiguousarray(x).ravel(order="K")
+            s = float(np.dot(flat, flat)) / (m * m)
+        else:
+            s = float(np.sum(np.square(x / m)))
+        if self.scale < m:
+            self.sumsq = s + self.sumsq * (self.scale / m) ** 2
+            self.scale = m
+        else:
+            self.sumsq += s * (m / self.scale) ** 2
+
+    def norm(self) -> float:
+        if not self.finite:
+            return float("inf")
+        return self.scale * float(np.sqrt(self.sumsq)) if self.scale > 0 else 0.0
+
+
+def _ssq_ratio(num: _Ssq, den: _Ssq) -> float:
+    if not num.finite or not den.finite:
+        return float("inf")
+    if den.scale == 0.0:
+        return 0.0 if num.scale == 0.0 else float("inf")
+    return (num.scale / den.scale) * float(np.sqrt(num.sumsq / den.sumsq))
+
+
+def potrf_residual_tiled(L2d: np.ndarray, A2d: np.ndarray, block: int = 4096) -> float:
+    """||A - L L^T||_F / ||A||_F in FP64 for n x n arrays (L2d: lower factor;
+    its strict upper triangle is ignored).  One lower block column of L L^T
+    is formed per step; each computed product entry (r, c), r >= c, is compared
+    with A(r, c) and, for r > c outside the diagonal block, with A(c, r)."""
+    n = A2d.shape[0]
+    num, den = _Ssq(), _Ssq()
+    for j0 in range(0, n, block):
+        j1 = min(n, j0 + block)
+        X = np.array(L2d[j0:, :j1], dtype=np.float64, order="F")  # rows j0..n, columns 0..j1
+        for c in range(j1 - j0):  # diagonal block: lower triangle only
+            X[:c, j0 + c] = 0.0
+        P = X @ X[: j1 - j0, :].T                           # (L L^T)[j0:n, j0:j1]
+        del X
+        D = P[: j1 - j0] - A2d[j0:j1, j0:j1]
+        num.add(D)
+        den.add(np.asarray(A2d[j0:j1, j0:j1], dtype=np.float64))
+        if j1 < n:
+            low = np.asarray(A2d[j1:, j0:j1], dtype=np.float64)
+            up = np.asarray(A2d[j0:j1, j1:], dtype=np.float64)
+            num.add(P[j1 - j0:] - low)
+            num.add(P[j1 - j0:].T - up)
+            den.add(low)
+            den.add(up)
+        del P
+    return _ssq_ratio(num, den)
+
+
+def getrf_residual_tiled(LU2d: np.ndarray, A2d: np.ndarray, ipiv, block: int = 4096) -> float:
+    """||P A - L U||_F / ||A||_F in FP64 for n x n arrays; ipiv 1-based LAPACK
+    pivots (an invalid pivot gives +inf, cpu_fp64_residual.h:157-163).  One
+    block column of L U is formed per step from the trapezoidal blocks of L
+    that can reach it."""
+    n = A2d.shape[0]
+    perm = ipiv_to_perm(ipiv, n)
+    if perm is None:
+        return float("inf")
+    num, den = _Ssq(), _Ssq()
+    for j0 in range(0, n, block):
+        j1 = min(n, j0 + block)
+        P = np.zeros((n, j1 - j0), dtype=np.float64)
+        for k0 in range(0, j1, block):
+            k1 = min(n, k0 + block)
+            Lk = np.array(LU2d[k0:, k0:k1], dtype=np.float64, order="F")  # rows k0..n
+            for c in range(k1 - k0):  # unit lower diagonal block
+                Lk[:c, c] = 0.0
+                Lk[c, c] = 1.0
+            Uk = np.array(LU2d[k0:k1, j0:j1], dtype=np.float64, order="F")
+            if k0 == j0:
+                for c in range(j1 - j0):  # upper diagonal block
+                    Uk[c + 1:, c] = 0.0
+            P[k0:] += Lk @ Uk
+            del Lk
+        PA = np.asarray(np.asarray(A2d[:, j0:j1])[perm], dtype=np.float64)
+        num.add(P - PA)
+        den.add(PA)
+        del P, PA
+    return _ssq_ratio(num, den)
+
+
 # --- reference loops restated in C (FP32 and FP64) -------------------------
 
 def double_blocked_potrf(A2d: np.ndarray, nb: int, b: int, syrk_k_tile: int = 0):
@@ -312,12 +434,11 @@ def pivot_divergence(A2d: np.ndarray, ipiv_a, ipiv_b):
         return None, None
     j = int(diff[0])
     n = A2d.shape[0]
-    M = np.array(A2d, dtype=np.float64)
     perm = np.arange(n)
     for r in range(j):
         p = a[r] - 1
         perm[r], perm[p] = perm[p], perm[r]
-    M = M[perm, :]
+    M = np.asarray(A2d[:, : j + 1], dtype=np.float64)[perm, :]  # only columns 0..j matter
     if j > 0:
         x = np.linalg.solve(M[:j, :j], M[:j, j])
         col = M[j:, j] - M[j:, :j] @ x

@@ -153,6 +153,42 @@ def test_blas_residual_agrees_with_c_oracle():
         assert a == pytest.approx(b, rel=1e-9)
 
 
+@pytest.mark.parametrize("n,block", [(1, 4), (7, 3), (96, 32), (301, 64), (300, 512)])
+def test_tiled_residuals_agree_with_c_oracle(n, block):
+    """The block-column BLAS residuals used at n >= 8192 give the C oracle's
+    value (both triangles of A compared, ragged last block, block > n)."""
+    A = oracle.spd_gram(n, 3)
+    L, info = oracle.double_blocked_potrf(A, 32, 8)
+    assert info == 0
+    L = np.asfortranarray(L)
+    a = oracle.potrf_residual(L.ravel(order="F"), np.asfortranarray(A).ravel(order="F"), n, n)
+    assert oracle.potrf_residual_tiled(L, A, block) == pytest.approx(a, rel=1e-9, abs=1e-300)
+    # a non-symmetric "original": the upper triangle is compared with (L L^T)^T
+    rng = np.random.default_rng(n)
+    A2 = (A + np.triu(rng.standard_normal((n, n)), 1).astype(np.float32) * 1e-3).astype(np.float32)
+    a2 = oracle.potrf_residual(L.ravel(order="F"), np.asfortranarray(A2).ravel(order="F"), n, n)
+    assert oracle.potrf_residual_tiled(L, A2, block) == pytest.approx(a2, rel=1e-9)
+    G = oracle.general_uniform(n, 4)
+    LU, ipiv, info = oracle.double_blocked_getrf(G, 32, 8)
+    a = oracle.getrf_residual(LU.ravel(order="F"), G.ravel(order="F"), ipiv, n, n)
+    assert oracle.getrf_residual_tiled(LU, G, ipiv, block) == pytest.approx(a, rel=1e-9,
+                                                                             abs=1e-300)
+
+
+def test_tiled_residual_edge_cases():
+    n = 40
+    G = oracle.general_uniform(n, 4)
+    LU, ipiv, _ = oracle.double_blocked_getrf(G, 16, 8)
+    bad = ipiv.copy()
+    bad[5] = 3  # ipiv[r] < r + 1: invalid
+    assert np.isinf(oracle.getrf_residual_tiled(LU, G, bad, 16))
+    LU2 = LU.copy()
+    LU2[30, 31] = np.nan
+    assert np.isinf(oracle.getrf_residual_tiled(LU2, G, ipiv, 16))
+    Z = np.zeros((n, n), np.float32)
+    assert oracle.potrf_residual_tiled(Z, Z, 16) == 0.0
+
+
 @pytest.mark.parametrize("n,nb,b", [(200, 64, 16), (300, 128, 32), (97, 40, 7)])
 def test_c_double_blocked_loops_match_lapack(n, nb, b):
     """The reference schedules restated in C reproduce host LAPACK's pivots and
