@@ -10,7 +10,8 @@ residual_ref.json  -- CPU FP64 residuals computed by the REFERENCE's own header
 lapack_f32.npz     -- host LAPACK (SciPy OpenBLAS) sgetrf pivots / info and
                       scaled residuals of sgetrf and spotrf on the seeded input
                       families (general U[-1,1) seed 1, SPD G G^T/n + I seed 0).
-Needs /root/reference only for residual_ref.json.
+Needs the reference checkout ($HDBF_REFERENCE_ROOT, else /root/reference) only
+for residual_ref.json.
 """
 from __future__ import annotations
 

@@ -100,3 +100,69 @@ def test_no_oracle_in_product_sources():
             txt = open(f).read()
             assert "import oracle" not in txt and "from oracle" not in txt, f
             assert "liboracle" not in txt, f
+
+
+# --- prototypes against the reference's (tests/golden/reference_prototypes.json)
+# Documented substitutions: rocblas_handle is this library's handle
+# (hdbf/rocblas_compat.h), hipStream_t is cudaStream_t, __half buffers travel
+# as void* (include/kernels/fp16_convert.h); every other type is unchanged.
+SUBST = {"hipStream_t": "cudaStream_t", "__half*": "void*", "const __half*": "const void*"}
+
+
+def _reference_prototypes():
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "reference_prototypes.json")) as f:
+        return json.load(f)
+
+
+def _our_prototypes():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_prototypes", os.path.join(ROOT, "tests", "golden", "make_prototypes.py"))
+    mp = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mp)
+    out = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True):
+        out.update(mp.prototypes(h))
+    return out
+
+
+def test_prototypes_match_reference_types():
+    """A C++ translation unit includes every header through rocblas_compat.h
+    and static_asserts that each entry point's type is the reference
+    prototype's type after the documented substitutions (argument count,
+    order and types; return type)."""
+    import shutil
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no host C++ compiler")
+    ref = _reference_prototypes()
+    lines = ["#include <type_traits>", "#include \"hdbf/rocblas_compat.h\""]
+    for h in sorted(glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True)):
+        lines.append(f'#include "{os.path.relpath(h, os.path.join(ROOT, "include"))}"')
+    for name, p in sorted(ref.items()):
+        types = ", ".join(SUBST.get(t, t) for t, _ in p["params"])
+        lines.append(f"static_assert(std::is_same<decltype(&{name}), {p['ret']} (*)({types})>::value,"
+                     f' "{name}: {p["file"]}:{p["line"]}");')
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "abi_check.cpp")
+        with open(src, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        r = subprocess.run([cxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                            "-I", "/usr/local/cuda/include", src], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+def test_prototypes_match_reference_parameter_names():
+    """Same parameter names in the same order as the reference (catches two
+    same-typed arguments swapped, which the type check cannot)."""
+    ref, ours = _reference_prototypes(), _our_prototypes()
+    bad = []
+    for name, p in ref.items():
+        assert name in ours, name
+        want = [n for _, n in p["params"]]
+        got = [n for _, n in ours[name]["params"]]
+        if want != got:
+            bad.append((name, want, got))
+    assert not bad, bad
