@@ -389,7 +389,15 @@ hdbf_status tc_launch(hdbf_context* ctx, int fmt, int M, int N, int K, const TcO
     args.err = ctx->dev_small + kSmallErr;
     const long long grid = (long long)args.tiles_m * ((N + TN - 1) / TN);
     if (grid > 0x7fffffffLL) return HDBF_STATUS_NOT_SUPPORTED;
-    const double flops = (split ? 3.0 : 1.0) * 2.0 * (double)M * N * K;
+    // Algorithmic flops: with lower_only only the entries row >= col of C are
+    // updated (the kernel skips tiles above the diagonal), so count
+    // sum over columns j < min(M, N) of (M - j) rows, as the FP32 GEMM does.
+    double entries = (double)M * N;
+    if (lower_only) {
+        const double d = (double)(M < N ? M : N);
+        entries = d * (double)M - d * (d - 1.0) / 2.0;
+    }
+    const double flops = (split ? 3.0 : 1.0) * 2.0 * entries * K;
     ProfScope prof(ctx, kClsTcGemm, flops,
                    (split ? 4.0 : 2.0) * ((double)M * K + (double)N * K) + 8.0 * M * N, M, N, K);
     if (split)
