@@ -18,8 +18,13 @@ e2e    = the same step through the C ABI starting from pinned HOST buffers:
 roofline = the dominant kernel (sgemm_sub_kernel, FP32 SIMT FFMA) from the
          library's per-launch event profiler over the timed region, against the
          FP32 SIMT peak (SMs x 128 lanes x 2 flop x max SM clock).
-cpu_baseline / --impl reference = host LAPACK spotrf + sgetrf (SciPy's OpenBLAS,
-         all host threads) on a bounded sample (n chosen so a step takes ~10 s).
+cpu_baseline = host LAPACK spotrf + sgetrf (SciPy's OpenBLAS, all host threads),
+         one step on the bench's own n=32768 inputs; the same leg then checks the
+         factors of the last timed step (parity object): CPU FP64 scaled
+         residuals <= 10 beside host LAPACK's, pivots vs host sgetrf.  The run
+         exits non-zero when that check fails.
+--impl reference = host LAPACK spotrf + sgetrf at the same n, all host threads,
+         as many full steps as fit in about six minutes (at least one).
 """
 from __future__ import annotations
 
@@ -109,21 +114,6 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- CPU LAPACK
-def cpu_lapack_step(n, seed_spd=0, seed_gen=1, inputs=None):
-    """One POTRF + GETRF step with host LAPACK; returns seconds (wall, LAPACK only)."""
-    import oracle  # CPU baseline leg only
-    from scipy.linalg import lapack
-    import numpy as np
-    A, G = inputs if inputs is not None else (oracle.spd_gram(n, seed_spd), oracle.general_uniform(n, seed_gen))
-    t0 = time.perf_counter()
-    c, info = lapack.spotrf(A, lower=1, clean=0, overwrite_a=0)
-    t1 = time.perf_counter()
-    lu, piv, info2 = lapack.sgetrf(G, overwrite_a=0)
-    t2 = time.perf_counter()
-    assert info == 0 and info2 == 0
-    return t1 - t0, t2 - t1
-
-
 def cpu_threads():
     try:
         from threadpoolctl import threadpool_info
@@ -135,44 +125,129 @@ def cpu_threads():
     return os.cpu_count(), None
 
 
-def cpu_sample_size(target_s=10.0, cap=32768):
-    """Largest n (multiple of 1024, <= cap) whose POTRF+GETRF step takes ~target_s."""
-    import numpy as np
-    import oracle
-    n0 = 2048
-    inputs = (np.asfortranarray(oracle.spd_gram(n0, 0)), np.asfortranarray(oracle.general_uniform(n0, 1)))
-    cpu_lapack_step(n0, inputs=inputs)  # warm
-    tp, tg = cpu_lapack_step(n0, inputs=inputs)
-    rate = (flops_potrf(n0) + flops_getrf(n0)) / max(tp + tg, 1e-6)
-    n = int((target_s * rate) ** (1.0 / 3.0))
-    n = max(2048, min(cap, n // 1024 * 1024))
-    return n
+def host_inputs(n):
+    """The bench's two input families built on the host (the reference arm has
+    no device): SPD A = G G^T / n + I with the FP64 product formed by dsyrk
+    (the same family as the device's FP64 GEMM; last-bit differences after the
+    FP32 rounding are possible), general G iid U[-1,1) (bit-identical)."""
+    import oracle  # CPU baseline leg only
+    from scipy.linalg import blas
+    G0 = oracle.general_uniform(n, 0).astype(np.float64)
+    S = blas.dsyrk(1.0 / n, G0, lower=1, trans=0)  # lower triangle of G0 G0^T / n
+    del G0
+    A = np.empty((n, n), dtype=np.float32, order="F")
+    w = 4096
+    for j0 in range(0, n, w):  # mirror the lower triangle, add I, round to FP32
+        j1 = min(n, j0 + w)
+        D = S[j0:j1, j0:j1]
+        D = np.tril(D) + np.tril(D, -1).T + np.eye(j1 - j0)
+        A[j0:j1, j0:j1] = D
+        A[j1:, j0:j1] = S[j1:, j0:j1]
+        A[j0:j1, j1:] = S[j1:, j0:j1].T
+    del S
+    return A, np.asfortranarray(oracle.general_uniform(n, 1))
 
 
-def cpu_baseline(steps=1, warmup=1, target_s=10.0):
-    import numpy as np
-    import oracle
-    n = cpu_sample_size(target_s)
-    A = np.asfortranarray(oracle.spd_gram(n, 0))
-    G = np.asfortranarray(oracle.general_uniform(n, 1))
-    for _ in range(warmup):
-        cpu_lapack_step(n, inputs=(A, G))
-    tot = 0.0
-    tp_sum = tg_sum = 0.0
+def lapack_pair(A, G):
+    """Host LAPACK spotrf(lower) + sgetrf on copies; returns (L, LU, ipiv, tp, tg)."""
+    from scipy.linalg import lapack
+    t0 = time.perf_counter()
+    c, info = lapack.spotrf(A, lower=1, clean=0, overwrite_a=0)
+    t1 = time.perf_counter()
+    lu, piv, info2 = lapack.sgetrf(G, overwrite_a=0)
+    t2 = time.perf_counter()
+    if info != 0 or info2 != 0:
+        raise SystemExit(f"host LAPACK failed: spotrf info {info}, sgetrf info {info2}")
+    return c, lu, (piv + 1).astype(np.int32), t1 - t0, t2 - t1
+
+
+def cpu_baseline_and_check(n, A, G, gpu):
+    """CPU baseline at the bench's own size, and the check of the timed factors.
+
+    Host LAPACK spotrf + sgetrf (SciPy's OpenBLAS, all host threads) run once
+    on the SAME FP32 inputs the GPU factored (copied from the device), timed
+    with the wall clock around each LAPACK call.  Then the oracle checks the
+    GPU's factors from the last timed step against the bound of the
+    reference's verify step (potrf_benchmark_common.cpp:294-344,
+    getrf_benchmark_common.cpp:54-72): the scaled CPU FP64 residual
+    ||A - LL^T||_F / (||A||_F n eps32) and ||PA - LU||_F / (||A||_F n eps32)
+    <= 10, beside host LAPACK's own residual on the same input, and the GPU
+    pivot sequence against sgetrf's (identical, or a first divergence at an
+    FP32 near-tie: the two candidates' |s| differ by < 1e-4 relative)."""
+    import oracle  # checker and CPU baseline leg only
+    thr, ver = cpu_threads()
+    Lh, LUh, pivh, tp, tg = lapack_pair(A, G)
+    value = (flops_potrf(n) + flops_getrf(n)) / (tp + tg) / 1e12
+    base = {"value": round(value, 4), "unit": UNIT, "cores": thr, "kind": "port",
+            "sample": (f"host LAPACK spotrf(lower)+sgetrf (SciPy OpenBLAS {ver}, {thr} threads, "
+                       f"{os.cpu_count()} host CPUs) on the bench's own n={n} inputs (copied "
+                       "from the device), 1 step"),
+            "n": n, "potrf_tflops": round(flops_potrf(n) / tp / 1e12, 4),
+            "getrf_tflops": round(flops_getrf(n) / tg / 1e12, 4),
+            "ms_per_step": round(1e3 * (tp + tg), 1)}
+    t0 = time.perf_counter()
+    rp_gpu = oracle.scaled(oracle.potrf_residual_tiled(gpu["L"], A), n)
+    rp_cpu = oracle.scaled(oracle.potrf_residual_tiled(Lh, A), n)
+    del Lh
+    rg_gpu = oracle.scaled(oracle.getrf_residual_tiled(gpu["LU"], G, gpu["ipiv"]), n)
+    rg_cpu = oracle.scaled(oracle.getrf_residual_tiled(LUh, G, pivh), n)
+    del LUh
+    j, gap = oracle.pivot_divergence(G, pivh, gpu["ipiv"])
+    ok = (rp_gpu <= 10.0 and rg_gpu <= 10.0 and (j is None or gap < oracle.NEAR_TIE)
+          and gpu["info"] == [0, 0])
+    check = {"ok": bool(ok), "n": n, "bound": 10.0, "eps": "2^-23",
+             "what": "factors of the last timed step vs the CPU FP64 oracle and host LAPACK",
+             "potrf_scaled_residual": round(rp_gpu, 5),
+             "potrf_scaled_residual_host_lapack": round(rp_cpu, 5),
+             "getrf_scaled_residual": round(rg_gpu, 5),
+             "getrf_scaled_residual_host_lapack": round(rg_cpu, 5),
+             "pivots_vs_sgetrf": ("identical" if j is None else
+                                  {"first_divergence": j, "rel_gap": gap,
+                                   "near_tie": bool(gap < oracle.NEAR_TIE)}),
+             "info": gpu["info"], "check_s": round(time.perf_counter() - t0, 1)}
+    return base, check
+
+
+def reference_arm(args):
+    """--impl reference: host LAPACK spotrf + sgetrf (the reference's CPU path
+    of its residual harness) at the bench's own size n, all host threads.
+    Warm-up is one small pair (it only starts the BLAS threads); then as many
+    of the requested steps as fit in about six minutes are timed, at least one,
+    each a full POTRF + GETRF of order n."""
+    thr, ver = cpu_threads()
+    n = args.n
+    Aw, Gw = host_inputs(2048)
+    lapack_pair(Aw, Gw)
+    t0 = time.perf_counter()
+    lapack_pair(Aw, Gw)
+    rate = (flops_potrf(2048) + flops_getrf(2048)) / (time.perf_counter() - t0)
+    A, G = host_inputs(n)
+    est = (flops_potrf(n) + flops_getrf(n)) / (2.0 * rate)  # larger orders run faster
+    steps = max(1, min(args.steps, int(360.0 / max(est, 1e-3))))
+    tot = tp_sum = tg_sum = 0.0
     for _ in range(steps):
-        tp, tg = cpu_lapack_step(n, inputs=(A, G))
+        _, _, _, tp, tg = lapack_pair(A, G)
         tp_sum += tp
         tg_sum += tg
     tot = tp_sum + tg_sum
-    thr, ver = cpu_threads()
     value = steps * (flops_potrf(n) + flops_getrf(n)) / tot / 1e12
-    return {"value": round(value, 4), "unit": UNIT, "cores": thr, "kind": "port",
-            "sample": (f"host LAPACK spotrf(lower)+sgetrf (SciPy OpenBLAS {ver}, {thr} threads) "
-                       f"on the same input families at n={n} (bounded sample of the n=32768 "
-                       f"workload), {steps} step(s) after {warmup} warm-up"),
+    return {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "steps_requested": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * tot / steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (same seeded input families, built on the host)",
+            "impl": "reference",
+            "config": {"workload": (f"host LAPACK spotrf(lower)+sgetrf at n={n} (the POTRF+GETRF "
+                                    f"workload of the GPU arm), {steps} full step(s)"), "n": n},
             "potrf_tflops": round(steps * flops_potrf(n) / tp_sum / 1e12, 4),
             "getrf_tflops": round(steps * flops_getrf(n) / tg_sum / 1e12, 4),
-            "n": n, "ms_per_step": round(1e3 * tot / steps, 2)}
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": thr, "kind": "port",
+                             "sample": (f"SciPy OpenBLAS {ver} spotrf+sgetrf, {thr} threads, "
+                                        f"n={n}, {steps} step(s) (of {args.steps} requested: "
+                                        "steps beyond a six-minute budget are not run), "
+                                        "warm-up one n=2048 pair")},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
 
 
 # ----------------------------------------------------------------- GPU arm
@@ -476,6 +551,109 @@ def batched_case(torch, hd, handle, reps=5):
             "worst_backward_error": worst_be, "eps": "2^-23"}
 
 
+# The reference's published K100 AI times (ms) of the same two algorithms
+# (POTRF DoubleBlock+KBSYRK, GETRF DB-LU+BatchedPivot+MGEMM), per order.
+REF_PUBLISHED_SWEEP_MS = {8192: {"potrf": 32.5}, 16384: {"potrf": 108.9, "getrf": 492.6},
+                          32768: {"potrf": 565.6, "getrf": 2152.1},
+                          49152: {"potrf": 1655.2, "getrf": 6651.2}}
+
+
+def sweep(args):
+    """Config-1 sweep (opt-in, ``--sweep``): POTRF on G G^T/n + I and pivoted
+    GETRF on U[-1,1) for each order, with the bench's blocks (clamped to n).
+    Per order: device time of each factorization (mean of ``--steps`` after
+    ``--warmup``), then the checker on the host -- host LAPACK spotrf/sgetrf on
+    the same FP32 inputs (timed: the CPU baseline at that order), CPU FP64
+    scaled residuals of both factorizations (<= 10), GPU pivots vs sgetrf's
+    (identical, or a first divergence at an FP32 near-tie).  One JSON line per
+    order, then a summary line; exits non-zero if any order fails."""
+    import torch
+    import hygondoubleblockedfactorizations_b200 as hd
+    import oracle  # checker and CPU baseline leg only
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    thr, ver = cpu_threads()
+    rows = []
+    for n in [int(x) for x in args.sweep_sizes.split(",")]:
+        handle = hd.Handle(stream.cuda_stream)
+        wl = Workload(torch, hd, n, handle, dict(DEFAULTS))
+        times = {}
+        for op in ("potrf", "getrf"):
+            src, dst = (wl.spd0, wl.spd) if op == "potrf" else (wl.gen0, wl.gen)
+            run = (lambda: wl.potrf(dst)) if op == "potrf" else (lambda: wl.getrf(dst, wl.ipiv))
+            ts = []
+            for r in range(args.warmup + args.steps):
+                dst.copy_(src)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                run()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if r >= args.warmup:
+                    ts.append(e0.elapsed_time(e1))
+            times[op] = sum(ts) / len(ts)
+        handle.check("sweep")
+        info = wl.info.cpu().tolist()
+        dev_err = handle.device_errors()
+        from scipy.linalg import lapack
+        row = {"n": n, "info": info, "device_errors": dev_err, "blocks": {
+            "potrf": [min(n, DEFAULTS["potrf_nb"]), DEFAULTS["potrf_b"]],
+            "getrf": [min(n, DEFAULTS["getrf_nb"]), DEFAULTS["getrf_b"]]}}
+        # POTRF: host copies, LAPACK, residuals (one matrix family at a time)
+        A = wl.spd0.cpu().numpy().reshape(n, n).T
+        L = wl.spd.cpu().numpy().reshape(n, n).T
+        t0 = time.perf_counter()
+        Lh, inf_h = lapack.spotrf(A, lower=1, clean=0, overwrite_a=0)
+        tp = time.perf_counter() - t0
+        rp = oracle.scaled(oracle.potrf_residual_tiled(L, A), n)
+        rph = oracle.scaled(oracle.potrf_residual_tiled(Lh, A), n)
+        del A, L, Lh
+        G = wl.gen0.cpu().numpy().reshape(n, n).T
+        LU = wl.gen.cpu().numpy().reshape(n, n).T
+        ipiv = wl.ipiv.cpu().numpy().copy()
+        del wl
+        handle.close()
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        LUh, pivh, inf_g = lapack.sgetrf(G, overwrite_a=0)
+        tg = time.perf_counter() - t0
+        pivh = (pivh + 1).astype(np.int32)
+        rg = oracle.scaled(oracle.getrf_residual_tiled(LU, G, ipiv), n)
+        rgh = oracle.scaled(oracle.getrf_residual_tiled(LUh, G, pivh), n)
+        del LU, LUh
+        j, gap = oracle.pivot_divergence(G, pivh, ipiv)
+        del G
+        ok = (info == [0, 0] and dev_err == 0 and rp <= 10.0 and rg <= 10.0
+              and (j is None or gap < oracle.NEAR_TIE))
+        pub = REF_PUBLISHED_SWEEP_MS.get(n, {})
+        row.update({
+            "ok": bool(ok),
+            "potrf_ms": round(times["potrf"], 3),
+            "potrf_tflops": round(flops_potrf(n) / (times["potrf"] / 1e3) / 1e12, 3),
+            "getrf_ms": round(times["getrf"], 3),
+            "getrf_tflops": round(flops_getrf(n) / (times["getrf"] / 1e3) / 1e12, 3),
+            "potrf_scaled_residual": round(rp, 5), "potrf_scaled_residual_host_lapack": round(rph, 5),
+            "getrf_scaled_residual": round(rg, 5), "getrf_scaled_residual_host_lapack": round(rgh, 5),
+            "pivots_vs_sgetrf": ("identical" if j is None else
+                                 {"first_divergence": j, "rel_gap": gap,
+                                  "near_tie": bool(gap < oracle.NEAR_TIE)}),
+            "cpu_baseline": {"potrf_ms": round(1e3 * tp, 1), "getrf_ms": round(1e3 * tg, 1),
+                             "potrf_tflops": round(flops_potrf(n) / tp / 1e12, 4),
+                             "getrf_tflops": round(flops_getrf(n) / tg / 1e12, 4),
+                             "cores": thr, "kind": "port",
+                             "sample": f"SciPy OpenBLAS {ver} spotrf+sgetrf, {thr} threads, 1 run"},
+            "reference_published_k100_ms": pub or None})
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+    bad = [r["n"] for r in rows if not r["ok"]]
+    print(json.dumps({"sweep": "config-1 FP32 POTRF + GETRF", "orders": [r["n"] for r in rows],
+                      "all_ok": not bad, "failed": bad, "steps": args.steps,
+                      "warmup": args.warmup, "eps": "2^-23", "bound": 10.0}), flush=True)
+    if bad:
+        raise SystemExit(f"sweep check failed at n={bad}")
+
+
 def gpu_index():
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     if vis and vis.split(",")[0].strip().isdigit():
@@ -550,6 +728,15 @@ def run_ours(args, rank, world):
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
     ms_max = float(t.item())
     info = wl.info.cpu().tolist()
+    # the last timed step's factors, kept for the check against the oracle
+    # (later legs reuse the device buffers)
+    factors = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        factors = {"L": wl.spd.cpu().numpy().reshape(n, n).T,
+                   "LU": wl.gen.cpu().numpy().reshape(n, n).T,
+                   "ipiv": wl.ipiv.cpu().numpy().copy(), "info": info,
+                   "A": wl.spd0.cpu().numpy().reshape(n, n).T,
+                   "G": wl.gen0.cpu().numpy().reshape(n, n).T}
 
     # per-op split (one extra untimed step, events between the two ops)
     e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -729,7 +916,7 @@ def run_ours(args, rank, world):
            "info": info, "gpu_launches": launches, "kernels": kernels,
            "roofline": roof, "clocks": clocks, "e2e": e2e, "mixed_ir": mixed,
            "batched": batched, "fp64": fp64}
-    return out, handle
+    return out, handle, factors
 
 
 def main():
@@ -744,6 +931,9 @@ def main():
     ap.add_argument("--skip-mixed", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--sweep", action="store_true",
+                    help="config-1 sweep with oracle checks instead of the bench line")
+    ap.add_argument("--sweep-sizes", default="4096,8192,16384,32768,49152")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -751,16 +941,11 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cb = cpu_baseline(steps=args.steps, warmup=args.warmup, target_s=8.0)
-        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["ms_per_step"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (same seeded input families)", "impl": "reference",
-                "config": {"workload": f"host LAPACK spotrf+sgetrf, bounded sample n={cb['n']} of the n={args.n} POTRF+GETRF workload", "n": cb["n"]},
-                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(reference_arm(args)), flush=True)
+        return
+
+    if args.sweep:
+        sweep(args)
         return
 
     if world > 1:
@@ -769,18 +954,25 @@ def main():
         import torch.distributed as tdist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    out, handle = run_ours(args, rank, world)
-    if rank == 0 and world == 1 and not args.skip_cpu:
-        out["cpu_baseline"] = {k: v for k, v in cpu_baseline(steps=1, warmup=1).items()
-                               if k in ("value", "unit", "cores", "kind", "sample", "n",
-                                        "potrf_tflops", "getrf_tflops")}
+    out, handle, factors = run_ours(args, rank, world)
+    parity_ok = True
+    if factors is not None:
+        handle.close()
+        handle = None
+        base, check = cpu_baseline_and_check(args.n, factors.pop("A"), factors.pop("G"), factors)
+        out["cpu_baseline"] = base
+        out["parity"] = check
+        parity_ok = check["ok"]
     if rank == 0:
         print(json.dumps(out), flush=True)
-    handle.close()
+    if handle is not None:
+        handle.close()
     if world > 1:
         import torch.distributed as tdist
         tdist.barrier()
         tdist.destroy_process_group()
+    if not parity_ok:
+        raise SystemExit("parity check of the timed factors failed (see the line's parity object)")
 
 
 if __name__ == "__main__":
