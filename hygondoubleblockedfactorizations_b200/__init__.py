@@ -42,9 +42,14 @@ _PROTOS = {
     "hdbf_profile_end": (c_int, [P, c_int, P, P, P, P]),
     "hdbf_profile_class_name": (ctypes.c_char_p, [c_int]),
     "hdbf_profile_num_classes": (c_int, []),
+    "hdbf_profile_num_stages": (c_int, []),
+    "hdbf_profile_stage_name": (ctypes.c_char_p, [c_int]),
+    "hdbf_profile_stages": (c_int, [P, c_int, P, P, P]),
     "hdbf_set_graph_mode": (c_int, [P, c_int]),
     "hdbf_set_panel_kernel": (c_int, [P, c_int]),
     "hdbf_set_lookahead": (c_int, [P, c_int]),
+    "hdbf_set_wait_limit": (c_int, [P, ctypes.c_uint]),
+    "hdbf_mixed_fallback_panels": (c_int, [P, ctypes.POINTER(c_int)]),
     # potrf
     "double_blocked_potrf": (None, [P, P, c_int, c_int, c_int, c_int, P]),
     "double_blocked_potrf_dbtrsm": (None, [P, P, c_int, c_int, c_int, c_int, P]),
@@ -150,7 +155,7 @@ class IrInfo(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("converged", c_int), ("final_precision", c_int),
                 ("factorizations", c_int), ("info", c_int), ("backward_error", c_double),
                 ("history", c_double * 64), ("factor_ms", c_double), ("refine_ms", c_double),
-                ("inner_iterations", c_int)]
+                ("inner_iterations", c_int), ("fallback_panels", c_int)]
 
 
 class HdbfError(RuntimeError):
@@ -234,6 +239,12 @@ class Handle:
         if st != 0:
             raise HdbfError(f"set_lookahead: {status_string(st)}")
 
+    def set_wait_limit(self, polls: int):
+        """Poll limit of the bounded device-side waits (0: the default)."""
+        st = lib().hdbf_set_wait_limit(self._h, int(polls))
+        if st != 0:
+            raise HdbfError(f"hdbf_set_wait_limit: {status_string(st)}")
+
     def set_graphs(self, enabled: bool):
         lib().hdbf_set_graph_mode(self._h, 1 if enabled else 0)
 
@@ -254,6 +265,19 @@ class Handle:
             raise HdbfError(f"profile_end: {status_string(st)}")
         return {L.hdbf_profile_class_name(i).decode(): (int(ln[i]), ms[i], fl[i], by[i])
                 for i in range(k) if ln[i]}
+
+    def profile_stages(self):
+        """Per driver stage of the last profiling interval (stages that ran,
+        in the library's stage order): {name: (calls, total_ms, flops)}."""
+        L = lib()
+        k = L.hdbf_profile_num_stages()
+        ms, fl = (c_double * k)(), (c_double * k)()
+        calls = (c_int * k)()
+        st = L.hdbf_profile_stages(self._h, k, ms, fl, calls)
+        if st != 0:
+            raise HdbfError(f"profile_stages: {status_string(st)}")
+        return {L.hdbf_profile_stage_name(i).decode(): (int(calls[i]), ms[i], fl[i])
+                for i in range(1, k) if calls[i]}
 
     def close(self):
         if self._h:

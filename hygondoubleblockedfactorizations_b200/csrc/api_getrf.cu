@@ -63,14 +63,22 @@ template <class T>
 hdbf_status trsm_llu_mode(hdbf_context* ctx, int rows, int cols, T* L, long long ldl,
                           T* B, long long ldb, bool iterative, int block)
 {
-    if (!iterative || block <= 0 || rows <= block) return trsm_llu(ctx, rows, cols, L, ldl, B, ldb);
+    if (!iterative || block <= 0 || rows <= block) {
+        StageScope sc(ctx, kStOuterTrsmDirect);
+        return trsm_llu(ctx, rows, cols, L, ldl, B, ldb);
+    }
     for (int r = 0; r < rows; r += block) {
         const int dr = std::min(block, rows - r);
-        HDBF_TRY(trsm_llu(ctx, dr, cols, at(L, ldl, r, r), ldl, B + r, ldb));
+        {
+            StageScope sc(ctx, kStOuterTrsmBlock);
+            HDBF_TRY(trsm_llu(ctx, dr, cols, at(L, ldl, r, r), ldl, B + r, ldb));
+        }
         const int tr = rows - r - dr;
-        if (tr > 0)
+        if (tr > 0) {
+            StageScope sc(ctx, kStOuterTrsmGemm);
             HDBF_TRY(gemm_sub(ctx, true, false, tr, cols, dr, at(L, ldl, r + dr, r), ldl, B + r,
                                ldb, B + r + dr, ldb));
+        }
     }
     return HDBF_STATUS_SUCCESS;
 }
@@ -147,7 +155,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
     inner_nb = std::min(inner_nb, outer_nb);
     const bool piv = mode != PivotMode::None;
     bool la = sizeof(T) == 4 && ctx->lookahead && mode != PivotMode::Immediate && n > outer_nb &&
-              n + inner_nb <= compose_running_max_m(ctx);
+              compose_running_fits(ctx, n, inner_nb);
     if (la && !ctx->la_stream) {
         // The stream and events are created outside any capture.
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -179,14 +187,19 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
         for (int inner = outer; inner < oend; inner += inner_nb) {
             const int isz = std::min(inner_nb, oend - inner);
             const int next = inner + isz;
-            HDBF_TRY(getrf_panel(ctx, n - inner, isz, at(A, lda, inner, inner), lda,
-                                 piv ? ipiv + inner : nullptr, inner, info, inner, piv, ws));
+            {
+                StageScope sc(ctx, kStPanel);
+                HDBF_TRY(getrf_panel(ctx, n - inner, isz, at(A, lda, inner, inner), lda,
+                                     piv ? ipiv + inner : nullptr, inner, info, inner, piv, ws));
+            }
             if (mode == PivotMode::Immediate) {
+                StageScope sc(ctx, kStPivotProp);
                 const int cb[2] = {0, next};
                 const int cc[2] = {inner, n - next};
                 HDBF_TRY(permute_cols(ctx, ws, A, lda, n, inner, ipiv + inner, isz, inner, info,
                                       cb, cc, 2));
             } else if (mode == PivotMode::Batched) {
+                StageScope sc(ctx, kStInnerPivot);
                 const int cb[2] = {outer, next};
                 const int cc[2] = {inner - outer, la ? 0 : oend - next};
                 HDBF_TRY(permute_cols(ctx, ws, A, lda, n, inner, ipiv + inner, isz, inner, info,
@@ -197,6 +210,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
                 const int hist = next - outer;
                 if (forked) wait_chunk(next);
                 if (la && mode == PivotMode::Batched) {  // the block's interchanges so far
+                    StageScope sc(ctx, kStInnerPivot);
                     HDBF_TRY(compose_running(ctx, ipiv + outer, inner - outer, hist, outer,
                                              n - outer, ws_perm(ctx), inner == outer, ws.src,
                                              ws.tgt, ws.count, info));
@@ -204,8 +218,12 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
                                          ws.count, std::min(n - outer, 2 * hist),
                                          ws_temp<T>(ws), ws.temp_cols));
                 }
-                HDBF_TRY(trsm_llu(ctx, hist, nsz, at(A, lda, outer, outer), lda,
-                                  at(A, lda, outer, next), lda));
+                {
+                    StageScope sc(ctx, kStInnerTrsm);
+                    HDBF_TRY(trsm_llu(ctx, hist, nsz, at(A, lda, outer, outer), lda,
+                                      at(A, lda, outer, next), lda));
+                }
+                StageScope sc(ctx, kStInnerGemm);
                 HDBF_TRY(gemm_nn_rows(ctx, n - next, nsz, hist, at(A, lda, next, outer), lda,
                                       at(A, lda, outer, next), lda, at(A, lda, next, next), lda,
                                       mode == PivotMode::Batched ? inner_gemm_m_tile : 0));
@@ -231,6 +249,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
         }
         nchunks = 0;
         if (mode == PivotMode::Batched) {  // outer pivot batch (:556-609)
+            StageScope sc(ctx, kStOuterPivot);
             if (outer > 0) {
                 const int cb[1] = {0};
                 const int cc[1] = {outer};
@@ -248,6 +267,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
             const int nsz = std::min(outer_nb, n - next);
             HDBF_TRY(trsm_llu_mode(ctx, next, nsz, A, lda, at(A, lda, 0, next), lda,
                                    iterative_outer, trsm_block));
+            StageScope sc(ctx, kStOuterGemm);
             if (la) {
                 const int panels = (nsz + inner_nb - 1) / inner_nb;
                 const int group = (panels + kLaEvents - 2) / (kLaEvents - 1);

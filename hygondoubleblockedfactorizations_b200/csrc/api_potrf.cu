@@ -120,14 +120,21 @@ hdbf_status potrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int nb, int b
             const int ps = inner + isz;
             const int rows = n - ps;
             T* Aii = at(A, lda, inner, inner);
-            HDBF_TRY(potrf_diag(ctx, isz, Aii, lda, info, inner));
-            if (use_dbtrsm) {
-                HDBF_TRY(dbtrsm_impl(ctx, Aii, lda, at(A, lda, ps, inner), lda, rows, isz, isz,
-                                     std::min(kPotrfDbTrsmMicroBlock, isz)));
-            } else {
-                HDBF_TRY(trsm_rlt(ctx, rows, isz, Aii, lda, at(A, lda, ps, inner), lda));
+            {
+                StageScope sc(ctx, kStPotrf);
+                HDBF_TRY(potrf_diag(ctx, isz, Aii, lda, info, inner));
+            }
+            {
+                StageScope sc(ctx, kStTrsm);
+                if (use_dbtrsm) {
+                    HDBF_TRY(dbtrsm_impl(ctx, Aii, lda, at(A, lda, ps, inner), lda, rows, isz,
+                                         isz, std::min(kPotrfDbTrsmMicroBlock, isz)));
+                } else {
+                    HDBF_TRY(trsm_rlt(ctx, rows, isz, Aii, lda, at(A, lda, ps, inner), lda));
+                }
             }
             if (ps < oend) {  // update_next_inner_panel (:210-249)
+                StageScope sc(ctx, kStInnerGemm);
                 const int pc = std::min(b, oend - ps);
                 const int k = ps - outer;
                 const bool mt = m_tile > 0 && rows > m_thr && k >= k_thr;
@@ -141,11 +148,15 @@ hdbf_status potrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int nb, int b
             const int nsz = std::min(nb, n - next);
             const int below = next + nsz;
             const int tk = (syrk_k_tile > 0 && syrk_k_tile < next) ? syrk_k_tile : next;
-            for (int k0 = 0; k0 < next; k0 += tk) {
-                const int kc = std::min(tk, next - k0);
-                HDBF_TRY(syrk_lower(ctx, nsz, kc, at(A, lda, next, k0), lda,
-                                    at(A, lda, next, next), lda));
+            {
+                StageScope sc(ctx, kStOuterSyrk);
+                for (int k0 = 0; k0 < next; k0 += tk) {
+                    const int kc = std::min(tk, next - k0);
+                    HDBF_TRY(syrk_lower(ctx, nsz, kc, at(A, lda, next, k0), lda,
+                                        at(A, lda, next, next), lda));
+                }
             }
+            StageScope sc(ctx, kStOuterGemm);
             HDBF_TRY(gemm_sub(ctx, false, false, n - below, nsz, next, at(A, lda, below, 0), lda,
                                at(A, lda, next, 0), lda, at(A, lda, below, next), lda));
         }

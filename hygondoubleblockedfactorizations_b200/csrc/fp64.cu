@@ -627,7 +627,7 @@ getf2_coop64_kernel(int m, int w, double* A, long long lda, int rpc, int* ipiv, 
             const double* sq = slot_of(par, q);
             unsigned polls = 0;
             while (ld_acquire_u32(reinterpret_cast<const unsigned*>(sq)) != seq) {
-                if (++polls > kSpinLimit) {
+                if (++polls > spin_limit_of(err)) {
                     atomicExch(err, kErrTimeout);
                     s_abort = 1;
                     break;

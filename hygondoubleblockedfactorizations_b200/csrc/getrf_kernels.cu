@@ -130,6 +130,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     const int nr = max(0, min(m, r0 + rpc) - r0);
     const int steps = min(m, w);
     const unsigned epoch = *reinterpret_cast<volatile unsigned*>(epoch_ptr);
+    const unsigned spin = spin_limit_of(err);
     auto slot_of = [&](int par, int q) {
         return scr + ((long long)par * kCoopMaxGrid + q) * kSlotWords;
     };
@@ -204,7 +205,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
             unsigned polls = 0;
             unsigned long long wv;
             while (((unsigned)((wv = ld_relaxed_u64(wq)) >> 16) & 0xffffu) != tag) {
-                if (++polls > kSpinLimit) {
+                if (++polls > spin) {
                     atomicExch(err, kErrTimeout);
                     s_abort = 1;
                     break;
@@ -252,7 +253,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                 unsigned polls = 0;
                 while ((unsigned)(wp >> 32) != want || (unsigned)(wo >> 32) != want ||
                        (fin && ((unsigned)(wl >> 32) != want || (unsigned)(wm >> 32) != want))) {
-                    if (++polls > kSpinLimit) {
+                    if (++polls > spin) {
                         atomicExch(err, kErrTimeout);
                         s_abort = 1;
                         break;
@@ -348,26 +349,204 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
 
 // ------------------------------------------------------------ compose swaps
 constexpr int kComposeThreads = 1024;
+constexpr int kComposeMaxK = 4096;  // swaps composed by the sorted-group kernels
 
+__host__ __device__ constexpr int pow2_at_least(int v)
+{
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// Block-wide ordered compaction: items q = 0 .. total-1 in order, item q
+// kept when pick(q, &s, &t) is true; kept items are written to src/tgt at
+// base + (rank among kept items).  Returns the new base (uniform).
+template <class Pick>
+__device__ int emit_ordered(int total, int base, int* src, int* tgt, int* warp_tot, int* s_chunk,
+                            Pick pick)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int q0 = 0; q0 < total; q0 += kComposeThreads) {
+        const int q = q0 + tid;
+        int s = 0, t = 0;
+        const bool moved = q < total && pick(q, &s, &t);
+        const unsigned ball = __ballot_sync(0xffffffffu, moved);
+        const int within = __popc(ball & ((1u << lane) - 1u));
+        if (lane == 0) warp_tot[warp] = __popc(ball);
+        __syncthreads();
+        if (tid == 0) {
+            int run = 0;
+            for (int wv = 0; wv < kComposeThreads / 32; ++wv) {
+                const int c = warp_tot[wv];
+                warp_tot[wv] = run;
+                run += c;
+            }
+            *s_chunk = run;
+        }
+        __syncthreads();
+        if (moved) {
+            src[base + warp_tot[warp] + within] = s;
+            tgt[base + warp_tot[warp] + within] = t;
+        }
+        base += *s_chunk;
+        __syncthreads();
+    }
+    return base;
+}
+
+// Composition of a LAPACK swap sequence without replaying it.  Step t
+// (t = 0 .. kk-1) exchanges the contents of position x_t = base + t with
+// position bt[t] >= x_t.  Position x_t is never touched after step t, and a
+// position p >= x_t is touched before step t only by the steps j < t with
+// bt[j] = p.  So, with the (bt, t) pairs sorted:
+//   prev(t) = the last j < t with bt[j] = bt[t]      (same-target group)
+//   g(u)    = the last j < u with bt[j] = x_u        (who filled x_u before step u)
+//   V(u)    = content of x_u just before step u = start(x_{root(u)}), root(u)
+//             the end of the chain u -> g(u) -> g(g(u)) ... (pointer jumping)
+// and the contents after the whole sequence are
+//   position x_t:                 prev(t) >= 0 ? V(prev(t)) : start(bt[t])
+//   target p >= base + kk (last t of its group): V(t).
+// Results: nv[t] (content of x_t), keys[s] the sorted pairs, root[u] the chain
+// ends; aux[t] holds prev(t).  start() must stay valid until the caller writes
+// the new contents.
+template <class Start>
+__device__ void compose_sorted(const int* bt, int kk, int base, int P, unsigned long long* keys,
+                               int* aux, int* root, int* nv, Start start)
+{
+    const int tid = threadIdx.x;
+    for (int s = tid; s < P; s += kComposeThreads)
+        keys[s] = s < kk ? ((unsigned long long)(unsigned)bt[s] << 32) | (unsigned)s : ~0ull;
+    for (int u = tid; u < kk; u += kComposeThreads) root[u] = -1;
+    __syncthreads();
+    // bitonic sort, ascending (b, t)
+    for (int size = 2; size <= P; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = tid; i < P / 2; i += kComposeThreads) {
+                const int lo = 2 * i - (i & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const unsigned long long a = keys[lo], b = keys[hi];
+                if ((a > b) == up) {
+                    keys[lo] = b;
+                    keys[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int s = tid; s < kk; s += kComposeThreads) {
+        const unsigned long long key = keys[s];
+        const int b = (int)(key >> 32), t = (int)(key & 0xffffffffu);
+        const bool has_prev = s > 0 && (int)(keys[s - 1] >> 32) == b;
+        aux[t] = has_prev ? (int)(keys[s - 1] & 0xffffffffu) : -1;
+        const int u = b - base;  // b is the swap-side position of step u
+        if (u < kk && t < u) {
+            const bool next_in = s + 1 < kk && (int)(keys[s + 1] >> 32) == b;
+            if (!next_in || (int)(keys[s + 1] & 0xffffffffu) == u) root[u] = t;
+        }
+    }
+    __syncthreads();
+    for (int u = tid; u < kk; u += kComposeThreads)
+        if (root[u] < 0) root[u] = u;
+    __syncthreads();
+    // Pointer jumping: every root[] value is an ancestor, so reading an entry
+    // another thread is updating in the same round is harmless; a round in
+    // which nothing changes has read only settled values.
+    for (;;) {
+        int changed = 0;
+        for (int u = tid; u < kk; u += kComposeThreads) {
+            const int r = root[u], rr = root[r];
+            if (rr != r) {
+                root[u] = rr;
+                changed = 1;
+            }
+        }
+        if (!__syncthreads_or(changed)) break;
+    }
+    for (int t = tid; t < kk; t += kComposeThreads) {
+        const int p = aux[t];
+        nv[t] = p >= 0 ? start(base + root[p]) : start(bt[t]);
+    }
+    __syncthreads();
+}
+
+// Shared-memory layout of the sorted-group kernels (after `lead` ints):
+// keys[P] (8-byte aligned), then bt, aux, root, nv (kk ints each).
+__host__ __device__ inline size_t compose_sorted_bytes(int lead, int kk)
+{
+    const size_t head = ((size_t)lead * sizeof(int) + 15) / 16 * 16;
+    return head + (size_t)pow2_at_least(kk < 1 ? 1 : kk) * 8 + 4 * (size_t)kk * sizeof(int);
+}
+
+// Swaps ipiv[0..k) (rows local after subtracting 1 + ipiv_minus) composed
+// into the row moves of A(0:m, :): rows [0, k) in order, then the distinct
+// pivot rows >= k in increasing order.  Touches O(k) rows only.
 __global__ void __launch_bounds__(kComposeThreads)
 compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m, int* src,
-                     int* tgt, int* count, int* gperm, int use_smem, int* info, int* err)
+                     int* tgt, int* count, int* info, int* err)
 {
-    // Shared layout (use_smem): perm[m] then the k pivots; otherwise perm
-    // lives in global scratch and the pivots are re-read from global memory.
+    extern __shared__ __align__(16) unsigned char craw[];
+    __shared__ int warp_tot[kComposeThreads / 32];
+    __shared__ int s_bad, s_chunk;
+    const int P = pow2_at_least(k);
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(craw);
+    int* bt = reinterpret_cast<int*>(keys + P);
+    int* aux = bt + k;
+    int* root = aux + k;
+    int* nv = root + k;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    for (int i = tid; i < k; i += kComposeThreads) {
+        const int b = ipiv[i] - 1 - ipiv_minus;
+        if (b < i || b >= m) s_bad = 1;
+        bt[i] = b;
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (tid == 0) {
+            *count = 0;
+            if (info) atomicExch(info, -1);
+            atomicExch(err, kErrBadPivot);
+        }
+        return;
+    }
+    compose_sorted(bt, k, 0, P, keys, aux, root, nv, [](int x) { return x; });
+    int base = emit_ordered(k, 0, src, tgt, warp_tot, &s_chunk, [&](int q, int* s, int* t) {
+        *s = nv[q];
+        *t = q;
+        return nv[q] != q;
+    });
+    base = emit_ordered(k, base, src, tgt, warp_tot, &s_chunk, [&](int q, int* s, int* t) {
+        const unsigned long long key = keys[q];
+        const int b = (int)(key >> 32);
+        if (b < k || (q + 1 < k && (int)(keys[q + 1] >> 32) == b)) return false;
+        *s = root[(int)(key & 0xffffffffu)];
+        *t = b;
+        return *s != b;
+    });
+    if (tid == 0) *count = base;
+}
+
+// The same composition by replaying the swaps in one thread, for sequences
+// longer than kComposeMaxK: perm[m] (shared memory, or global scratch when
+// it does not fit), then the same move order.
+__global__ void __launch_bounds__(kComposeThreads)
+compose_swaps_serial_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m,
+                            int* src, int* tgt, int* count, int* gperm, int use_smem, int* info,
+                            int* err)
+{
     extern __shared__ int sperm[];
     __shared__ int warp_tot[kComposeThreads / 32];
-    __shared__ int s_base, s_bad, s_chunk;
+    __shared__ int s_bad, s_chunk;
     int* perm = use_smem ? sperm : gperm;
-    int* piv = use_smem ? sperm + m : nullptr;
     const int tid = threadIdx.x;
-    if (tid == 0) { s_bad = 0; s_base = 0; }
+    if (tid == 0) s_bad = 0;
     __syncthreads();
     for (int q = tid; q < m; q += kComposeThreads) perm[q] = q;
     for (int i = tid; i < k; i += kComposeThreads) {
         const int b = ipiv[i] - 1 - ipiv_minus;
         if (b < i || b >= m) s_bad = 1;
-        if (piv) piv[i] = b;
     }
     __syncthreads();
     if (s_bad) {
@@ -378,84 +557,58 @@ compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m,
         }
         return;
     }
-    // The swap sequence itself is inherently ordered: one thread replays it.
     if (tid == 0) {
         for (int i = 0; i < k; ++i) {
-            const int b = piv ? piv[i] : ipiv[i] - 1 - ipiv_minus;
-            if (b != i) {
-                const int t = perm[i];
-                perm[i] = perm[b];
-                perm[b] = t;
-            }
+            const int b = ipiv[i] - 1 - ipiv_minus;
+            const int t = perm[i];
+            perm[i] = perm[b];
+            perm[b] = t;
         }
     }
     __syncthreads();
-    // Moves: rows [0, k) in order (ordered block scan), then the distinct
-    // pivot rows >= k (each claimed once by flipping its entry negative).
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int q0 = 0; q0 < k; q0 += kComposeThreads) {
-        const int q = q0 + tid;
-        const int s = (q < k) ? perm[q] : q;
-        const bool moved = (q < k) && (s != q);
-        const unsigned ball = __ballot_sync(0xffffffffu, moved);
-        const int within = __popc(ball & ((1u << lane) - 1u));
-        if (lane == 0) warp_tot[warp] = __popc(ball);
-        __syncthreads();
-        if (tid == 0) {
-            int run = 0;
-            for (int wv = 0; wv < kComposeThreads / 32; ++wv) {
-                const int t = warp_tot[wv];
-                warp_tot[wv] = run;
-                run += t;
-            }
-            s_chunk = run;
-        }
-        __syncthreads();
-        if (moved) {
-            const int pos = s_base + warp_tot[warp] + within;
-            src[pos] = s;
-            tgt[pos] = q;
-        }
-        __syncthreads();
-        if (tid == 0) s_base += s_chunk;
-        __syncthreads();
-    }
-    for (int i = tid; i < k; i += kComposeThreads) {
-        const int b = piv ? piv[i] : ipiv[i] - 1 - ipiv_minus;
-        if (b < k) continue;
-        const int s = atomicExch(&perm[b], -1);  // claim position b once
-        if (s >= 0 && s != b) {
-            const int pos = atomicAdd(&s_base, 1);
-            src[pos] = s;
-            tgt[pos] = b;
-        }
-    }
-    __syncthreads();
-    if (tid == 0) *count = s_base;
+    int base = emit_ordered(k, 0, src, tgt, warp_tot, &s_chunk, [&](int q, int* s, int* t) {
+        *s = perm[q];
+        *t = q;
+        return perm[q] != q;
+    });
+    // pivot rows >= k: each distinct row once, in increasing row order
+    base = emit_ordered(m - k, base, src, tgt, warp_tot, &s_chunk, [&](int q, int* s, int* t) {
+        *s = perm[k + q];
+        *t = k + q;
+        return perm[k + q] != k + q;
+    });
+    if (tid == 0) *count = base;
 }
 
-// Running composition for the GETRF look-ahead: the block's permutation is
-// kept in global memory between launches and staged in shared memory with the
-// new pivots; only the new swaps are replayed (one thread, inherently
-// ordered), then every displaced row becomes a move, in increasing target
-// order.
+// Running composition for the GETRF look-ahead: the block's permutation pos[m]
+// (position -> source row, kept in global memory between launches) is staged
+// in shared memory, the new swaps ipiv[k0..k1) are composed on top of it by
+// the sorted-group method, and every displaced row of the block becomes a
+// move, in increasing target order.
 __global__ void __launch_bounds__(kComposeThreads)
 compose_running_kernel(const int* __restrict__ ipiv, int k0, int k1, int ipiv_minus, int m,
                        int* pos, int init, int* src, int* tgt, int* count, int* info, int* err)
 {
-    extern __shared__ int sp[];  // pos[m], then the pivots of [k0, k1)
+    extern __shared__ __align__(16) unsigned char craw[];
     __shared__ int warp_tot[kComposeThreads / 32];
-    __shared__ int s_base, s_bad, s_chunk;
-    int* piv = sp + m;
+    __shared__ int s_bad, s_chunk;
+    const int kk = k1 - k0;
+    const int P = pow2_at_least(kk < 1 ? 1 : kk);
+    int* sp = reinterpret_cast<int*>(craw);
+    unsigned long long* keys =
+        reinterpret_cast<unsigned long long*>(craw + ((size_t)m * sizeof(int) + 15) / 16 * 16);
+    int* bt = reinterpret_cast<int*>(keys + P);
+    int* aux = bt + kk;
+    int* root = aux + kk;
+    int* nv = root + kk;
     const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) { s_bad = 0; s_base = 0; }
+    if (tid == 0) s_bad = 0;
     __syncthreads();
     for (int q = tid; q < m; q += kComposeThreads) sp[q] = init ? q : pos[q];
-    for (int i = k0 + tid; i < k1; i += kComposeThreads) {
-        const int b = ipiv[i] - 1 - ipiv_minus;
-        if (b < i || b >= m) s_bad = 1;
-        piv[i - k0] = b;
+    for (int t = tid; t < kk; t += kComposeThreads) {
+        const int b = ipiv[k0 + t] - 1 - ipiv_minus;
+        if (b < k0 + t || b >= m) s_bad = 1;
+        bt[t] = b;
     }
     __syncthreads();
     if (s_bad) {
@@ -466,46 +619,29 @@ compose_running_kernel(const int* __restrict__ ipiv, int k0, int k1, int ipiv_mi
         }
         return;
     }
-    if (tid == 0) {
-        for (int i = k0; i < k1; ++i) {
-            const int b = piv[i - k0];
-            if (b != i) {
-                const int t = sp[i];
-                sp[i] = sp[b];
-                sp[b] = t;
-            }
-        }
-    }
-    __syncthreads();
-    for (int q0 = 0; q0 < m; q0 += kComposeThreads) {
-        const int q = q0 + tid;
-        const int s = q < m ? sp[q] : q;
-        if (q < m) pos[q] = s;
-        const bool moved = q < m && s != q;
-        const unsigned ball = __ballot_sync(0xffffffffu, moved);
-        const int within = __popc(ball & ((1u << lane) - 1u));
-        if (lane == 0) warp_tot[warp] = __popc(ball);
-        __syncthreads();
-        if (tid == 0) {
-            int run = 0;
-            for (int wv = 0; wv < kComposeThreads / 32; ++wv) {
-                const int t = warp_tot[wv];
-                warp_tot[wv] = run;
-                run += t;
-            }
-            s_chunk = run;
+    if (kk > 0) {
+        compose_sorted(bt, kk, k0, P, keys, aux, root, nv, [&](int x) { return sp[x]; });
+        // final contents of the targets beyond the swapped rows (aux reused)
+        for (int s = tid; s < kk; s += kComposeThreads) {
+            const unsigned long long key = keys[s];
+            const int b = (int)(key >> 32);
+            const bool last = !(s + 1 < kk && (int)(keys[s + 1] >> 32) == b);
+            aux[s] = (last && b >= k1) ? sp[k0 + root[(int)(key & 0xffffffffu)]] : -1;
         }
         __syncthreads();
-        if (moved) {
-            const int o = s_base + warp_tot[warp] + within;
-            src[o] = s;
-            tgt[o] = q;
+        for (int t = tid; t < kk; t += kComposeThreads) {
+            sp[k0 + t] = nv[t];
+            if (aux[t] >= 0) sp[(int)(keys[t] >> 32)] = aux[t];
         }
-        __syncthreads();
-        if (tid == 0) s_base += s_chunk;
         __syncthreads();
     }
-    if (tid == 0) *count = s_base;
+    for (int q = tid; q < m; q += kComposeThreads) pos[q] = sp[q];
+    const int base = emit_ordered(m, 0, src, tgt, warp_tot, &s_chunk, [&](int q, int* s, int* t) {
+        *s = sp[q];
+        *t = q;
+        return sp[q] != q;
+    });
+    if (tid == 0) *count = base;
 }
 
 // ------------------------------------------------------------ apply moves
@@ -600,6 +736,8 @@ void configure_getrf_kernels(hdbf_context* ctx)
                          (int)cap8);
     cudaFuncSetAttribute(compose_swaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)cap4);
+    cudaFuncSetAttribute(compose_swaps_serial_kernel,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap4);
     cudaFuncSetAttribute(apply_moves_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)cap4);
     cudaFuncSetAttribute(compose_running_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -657,32 +795,41 @@ hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_mi
                           int* src, int* tgt, int* count, int* gperm, int* info)
 {
     if (k <= 0 || m <= 0) return HDBF_STATUS_SUCCESS;
-    const size_t smem = ((size_t)m + (size_t)k) * sizeof(int);
+    if (k > m) return HDBF_STATUS_INVALID_VALUE;
     const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
+    if (k <= kComposeMaxK) {
+        const size_t smem = compose_sorted_bytes(0, k);
+        ProfScope prof(ctx, kClsCompose, 0.0, 12.0 * k);
+        compose_swaps_kernel<<<1, kComposeThreads, smem, ctx->stream>>>(
+            ipiv, k, ipiv_minus, m, src, tgt, count, info, ctx->dev_small + kSmallErr);
+        ctx->launches++;
+        return last_cuda(ctx);
+    }
+    const size_t smem = (size_t)m * sizeof(int);
     const int use_smem = smem <= cap ? 1 : 0;
     if (!use_smem && !gperm) return HDBF_STATUS_INVALID_VALUE;
     ProfScope prof(ctx, kClsCompose, 0.0, 4.0 * k + 8.0 * m);
-    compose_swaps_kernel<<<1, kComposeThreads, use_smem ? smem : 0, ctx->stream>>>(
+    compose_swaps_serial_kernel<<<1, kComposeThreads, use_smem ? smem : 0, ctx->stream>>>(
         ipiv, k, ipiv_minus, m, src, tgt, count, gperm, use_smem, info,
         ctx->dev_small + kSmallErr);
     ctx->launches++;
     return last_cuda(ctx);
 }
 
-int compose_running_max_m(hdbf_context* ctx)
+bool compose_running_fits(hdbf_context* ctx, int m, int kk)
 {
     const size_t cap = ctx->max_smem_optin > 4096 ? ctx->max_smem_optin - 4096 : 0;
-    return (int)(cap / sizeof(int));  // block height + new swaps
+    return kk >= 0 && kk <= kComposeMaxK && compose_sorted_bytes(m, kk) <= cap;
 }
 
 hdbf_status compose_running(hdbf_context* ctx, const int* ipiv, int k0, int k1, int ipiv_minus,
                             int m, int* pos, bool init, int* src, int* tgt, int* count, int* info)
 {
     if (m <= 0) return HDBF_STATUS_SUCCESS;
-    if (m + (k1 - k0) > compose_running_max_m(ctx) || k0 < 0 || k1 < k0 || k1 > m)
+    if (k0 < 0 || k1 < k0 || k1 > m || !compose_running_fits(ctx, m, k1 - k0))
         return HDBF_STATUS_INVALID_VALUE;
-    ProfScope prof(ctx, kClsCompose, 0.0, 4.0 * (k1 - k0) + 12.0 * m);
-    const size_t smem = ((size_t)m + (size_t)(k1 - k0)) * sizeof(int);
+    ProfScope prof(ctx, kClsCompose, 0.0, 12.0 * (k1 - k0) + 12.0 * m);
+    const size_t smem = compose_sorted_bytes(m, k1 - k0);
     compose_running_kernel<<<1, kComposeThreads, smem, ctx->stream>>>(
         ipiv, k0, k1, ipiv_minus, m, pos, init ? 1 : 0, src, tgt, count, info,
         ctx->dev_small + kSmallErr);

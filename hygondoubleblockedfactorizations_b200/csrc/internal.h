@@ -30,12 +30,34 @@ enum KernelClass {
     kClsPotrfBlock = 16, // potrf_block_kernel (cooperative diagonal-block Cholesky)
     kNumClasses = 17
 };
+// Algorithm stages of the double-blocked drivers for the per-stage profile
+// (hdbf_profile_stages), named as the reference's stage profilers name them
+// (src/potrf/profile_double_blocked_potrf.cpp, src/getrf/getrf_batched_pivot_internal.h).
+enum Stage {
+    kStNone = 0,
+    kStPotrf,            // "POTRF": diagonal-block Cholesky
+    kStTrsm,             // "TRSM": panel TRSM of the Cholesky
+    kStInnerGemm,        // "Inner GEMM"
+    kStOuterSyrk,        // "Outer SYRK"
+    kStOuterGemm,        // "Outer GEMM"
+    kStPanel,            // "Panel GETRF"
+    kStPivotProp,        // "Pivot propagation" (immediate pivoting)
+    kStInnerPivot,       // "Inner pivot batch"
+    kStInnerTrsm,        // "Inner TRSM"
+    kStOuterPivot,       // "Outer pivot batch"
+    kStOuterTrsmBlock,   // "Outer TRSM block"
+    kStOuterTrsmGemm,    // "Outer TRSM GEMM"
+    kStOuterTrsmDirect,  // "Outer TRSM direct"
+    kNumStages
+};
 struct ProfRec {
     int cls;
     cudaEvent_t a, b;
     double flops;
     double bytes;
     int m = 0, n = 0, k = 0;  // problem shape (GEMM launches)
+    int stage = 0;            // Stage active when the launch was enqueued
+    unsigned call = 0;        // which entry into that stage (StageScope instance)
 };
 struct GraphEntry {
     std::vector<long long> key;
@@ -69,6 +91,18 @@ struct hdbf_context {
     cudaEvent_t la_ev[hdbf::kLaEvents] = {};
     bool la_used = false;    // the graph being captured forked onto la_stream
     bool no_skinny = false;  // keep GEMMs off the shared split-K scratch
+    unsigned spin_limit = 0; // hdbf_set_wait_limit (0: default)
+    // Conditional launches (RunIf): while set, the FP32 GEMM and the
+    // diagonal-block kernel run only when *run_if != 0 (read on the device).
+    const int* run_if = nullptr;
+    // Device counter of panels the last mixed Cholesky rebuilt in FP32.
+    unsigned* mixed_fallbacks = nullptr;
+    // Stage attribution of profiled launches (StageScope) and the per-stage
+    // split of the last profiling interval (hdbf_profile_stages).
+    int stage = 0;
+    unsigned stage_call = 0, stage_seq = 0;
+    double stage_ms[32] = {}, stage_flops[32] = {};
+    int stage_calls[32] = {};
     // Workspace arena (grown on demand outside stream capture).
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -102,6 +136,7 @@ namespace hdbf {
 
 // Layout of hdbf_context::dev_small (ints).
 constexpr int kSmallErr = 0;       // device error word (timeouts, invalid pivots)
+constexpr int kSmallSpin = 8;        // bounded-wait poll limit of the handle (0: kSpinLimit)
 constexpr int kSmallMoveCount = 12;  // move count of the last composed permutation
 constexpr int kSmallEpoch = 16;      // panel-kernel exchange epoch
 constexpr int kSmallDone = 20;       // panel-kernel finished-CTA counter
@@ -113,8 +148,35 @@ constexpr int kSmallInts = 64;
 constexpr int kErrTimeout = 1;
 constexpr int kErrBadPivot = 2;
 
-// Bounded-wait poll limit for grid barriers (~0.5 s with back-off).
+// Default bounded-wait poll limit for grid barriers (~0.5 s with back-off).
 constexpr unsigned kSpinLimit = 1u << 22;
+
+#ifdef __CUDACC__
+// Per-panel power-of-two scale of the 16-bit shadows, from the panel's max |x|
+// given as FP32 bits (written by an atomicMax over the panel): s = 2^k with
+// max * s in [128, 256); 1 for a zero or non-finite max; k clamped to
+// [-60, 60].  Exact (built from the exponent bits), so the converting kernel
+// and the GEMM epilogue that undoes it agree bit for bit.
+__device__ __forceinline__ int panel_scale_exp(unsigned maxbits)
+{
+    const int e = (int)((maxbits >> 23) & 0xffu);
+    if (maxbits == 0u || e == 0xff) return 0;
+    const int k = e == 0 ? 60 : 7 - (e - 127);
+    return k < -60 ? -60 : (k > 60 ? 60 : k);
+}
+__device__ __forceinline__ float pow2f_exact(int k)
+{
+    return __uint_as_float((unsigned)(127 + k) << 23);
+}
+
+// The handle's poll limit, read at kernel start from the small device block
+// whose error word `err` points at (hdbf_set_wait_limit).
+__device__ __forceinline__ unsigned spin_limit_of(const int* err)
+{
+    const unsigned v = *reinterpret_cast<const volatile unsigned*>(err + (kSmallSpin - kSmallErr));
+    return v ? v : kSpinLimit;
+}
+#endif
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -128,6 +190,39 @@ public:
 private:
     hdbf_context* ctx_;
     int idx_ = -1;
+};
+
+// RAII: launches enqueued while it lives are attributed to `stage` (one
+// "call" of that stage per scope).
+class StageScope {
+public:
+    StageScope(hdbf_context* ctx, int stage)
+        : ctx_(ctx), prev_(ctx->stage), prev_call_(ctx->stage_call)
+    {
+        ctx->stage = stage;
+        ctx->stage_call = ++ctx->stage_seq;
+    }
+    ~StageScope()
+    {
+        ctx_->stage = prev_;
+        ctx_->stage_call = prev_call_;
+    }
+private:
+    hdbf_context* ctx_;
+    int prev_;
+    unsigned prev_call_;
+};
+
+// RAII: launches of the conditional-capable kernels (FP32 GEMM, diagonal-block
+// Cholesky, block-column restore) enqueued while it lives do their work only
+// if *flag != 0 when they run; the skinny GEMM path is not taken meanwhile.
+class RunIf {
+public:
+    RunIf(hdbf_context* ctx, const int* flag) : ctx_(ctx), prev_(ctx->run_if) { ctx->run_if = flag; }
+    ~RunIf() { ctx_->run_if = prev_; }
+private:
+    hdbf_context* ctx_;
+    const int* prev_;
 };
 
 // Make sure the workspace holds at least `bytes`; returns nullptr and sets
@@ -252,20 +347,25 @@ hdbf_status getf2_cluster(hdbf_context* ctx, int m, int w, float* A, long long l
 int configure_cluster_panel(hdbf_context* ctx);
 
 // Compose LAPACK swaps  row (i) <-> row (ipiv[i]-1-ipiv_minus), i in [0,k),
-// over local rows [0, m) into (src, tgt, *count) moves.
+// over local rows [0, m) into (src, tgt, *count) moves (at most 2k): rows
+// [0, k) in order, then the distinct pivot rows >= k in increasing order.
+// k <= 4096 runs without replaying the swaps (sorted-group composition, O(k)
+// rows touched); longer sequences are replayed by one thread over perm[m]
+// (gperm when m ints do not fit in shared memory).
 hdbf_status compose_swaps(hdbf_context* ctx, const int* ipiv, int k, int ipiv_minus, int m,
                           int* src, int* tgt, int* count, int* gperm, int* info);
 // A[tgt[i], c] = old A[src[i], c] for c < ncols, i < *count (<= max_moves).
 // Running composition: pos (m ints, row i of the block holds original row
 // pos[i]) is reset to the identity when init is set, then the LAPACK swaps
 // ipiv[k0, k1) (1-based, minus ipiv_minus gives rows local to the block) are
-// replayed into it, and every i with pos[i] != i becomes a move (pos[i] -> i),
+// composed onto it, and every i with pos[i] != i becomes a move (pos[i] -> i),
 // in increasing i.  Fails (count 0, info -1) on a pivot outside [i, m).
 hdbf_status compose_running(hdbf_context* ctx, const int* ipiv, int k0, int k1, int ipiv_minus,
                             int m, int* pos, bool init, int* src, int* tgt, int* count,
                             int* info);
-// Largest block height + swap count compose_running holds in shared memory.
-int compose_running_max_m(hdbf_context* ctx);
+// Whether compose_running takes a block of height m and kk new swaps (its
+// shared memory holds pos[m] and the sorted-group arrays; kk <= 4096).
+bool compose_running_fits(hdbf_context* ctx, int m, int kk);
 hdbf_status apply_moves(hdbf_context* ctx, float* A, long long lda, int ncols,
                         const int* src, const int* tgt, const int* count, int max_moves,
                         float* temp, long long temp_cols);
@@ -281,23 +381,34 @@ struct TcOperand {
 constexpr int kFmtF16 = 0;   // IEEE binary16
 constexpr int kFmtBF16 = 1;  // bfloat16
 // C(M x N, FP32 column-major) -= scale * A * B^T on the tensor cores.
+// Optional device scales (sa_max / sb_max: panel max bits, see
+// panel_scale_exp): the epilogue then uses scale / (s_a s_b).
 hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
-                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only);
+                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only,
+                        const unsigned* sa_max = nullptr, const unsigned* sb_max = nullptr);
 // C -= scale * (A B^T + A Blo^T + Alo B^T): the split-precision product in one
 // launch (hi/lo operands share row/K origins), one FP32 accumulator in TMEM.
 hdbf_status tc_gemm_sub_split(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
                               const TcOperand& Alo, const TcOperand& B, const TcOperand& Blo,
-                              float* C, long long ldc, float scale, bool lower_only);
+                              float* C, long long ldc, float scale, bool lower_only,
+                              const unsigned* sa_max = nullptr, const unsigned* sb_max = nullptr);
 void configure_tc_kernels(hdbf_context* ctx);
 // dst(r, k) = round16(s * src(r, k)) for an rows x cols FP32 column-major block
 // into a K-major (row-major, ldd elements) 16-bit block; `hi_lo` additionally
 // writes the rounding residual round16(s*src - hi) into lo (may be null).
+// smax (optional): device max bits of the panel; the scale is then
+// 2^panel_scale_exp(*smax) instead of s.
 hdbf_status convert_transpose16(hdbf_context* ctx, int fmt, int rows, int cols, const float* src,
-                                long long lds, void* hi, void* lo, long long ldd, float s);
+                                long long lds, void* hi, void* lo, long long ldd, float s,
+                                const unsigned* smax = nullptr);
 // dst[c * ldd + r] = round16(s * src[c * lds + r]): same layout (column-major
 // FP32 -> "column = K-major row" 16-bit), with optional residual.
 hdbf_status convert_direct16(hdbf_context* ctx, int fmt, int rows, int cols, const float* src,
-                             long long lds, void* hi, void* lo, long long ldd, float s);
+                             long long lds, void* hi, void* lo, long long ldd, float s,
+                             const unsigned* smax = nullptr);
+// *slot = FP32 bits of max |A(r, c)| over rows x cols (slot cleared first).
+hdbf_status panel_absmax(hdbf_context* ctx, const float* A, long long lda, int rows, int cols,
+                         unsigned* slot);
 
 // Auxiliary kernels.
 hdbf_status fill_uniform(hdbf_context* ctx, float* x, size_t count, uint64_t seed,

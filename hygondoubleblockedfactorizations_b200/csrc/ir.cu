@@ -365,8 +365,12 @@ public:
             cudaGetLastError();
             return HDBF_STATUS_CUDA_ERROR;
         }
+        fallbacks_ = 0;
+        if (spd_ && prec != HDBF_PREC_FP32) HDBF_TRY(hdbf_mixed_fallback_panels(ctx_, &fallbacks_));
         return HDBF_STATUS_SUCCESS;
     }
+    // Cholesky panels the last factorization rebuilt in FP32 (panel fallback).
+    int fallbacks() const { return fallbacks_; }
 
     // d = A^{-1} v with the FP32 factors; v scaled column-wise by nrm.
     hdbf_status correction(const double* V, long long ldv, bool accumulate)
@@ -506,6 +510,7 @@ private:
     const double* A_;
     long long lda_;
     int n_, nrhs_;
+    int fallbacks_ = 0;
     const double* B_;
     long long ldb_;
     double* X_;
@@ -561,11 +566,13 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
         st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
         info.factorizations = 1;
         while (st == HDBF_STATUS_SUCCESS && hinfo != 0 && escalate && next_precision(cur) >= 0) {
-            cur = next_precision(cur);  // FP32-panel fallback on a failed factorization
+            // the panel fallback could not save it: refactor at the next precision
+            cur = next_precision(cur);
             st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
             info.factorizations++;
         }
         info.info = hinfo;
+        info.fallback_panels = solver.fallbacks();
         if (st == HDBF_STATUS_SUCCESS && hinfo == 0)
             st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });
         double prev = INFINITY;
@@ -597,6 +604,7 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
                     st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo2); });
                     info.factorizations++;
                     info.info = hinfo2;
+                    info.fallback_panels = solver.fallbacks();
                     if (hinfo2 != 0) break;
                     stalls = 0;
                 } else if (++stalls >= 2) {
@@ -683,6 +691,7 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
         st = timed(&info.factor_ms, [&] { return solver.factor(prec, &hinfo); });
         info.factorizations = 1;
         info.info = hinfo;
+        info.fallback_panels = solver.fallbacks();
     }
     if (st == HDBF_STATUS_SUCCESS && hinfo == 0)
         st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });

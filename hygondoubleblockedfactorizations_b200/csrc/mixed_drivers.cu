@@ -27,16 +27,11 @@
 namespace hdbf {
 
 size_t mixed_base_bytes(int n, int b);
+size_t mixed_slots_offset(int n, int b);
 
 namespace {
 
 inline long long pad8(long long x) { return (x + 7) / 8 * 8; }
-inline long long fbits(float f)
-{
-    unsigned int u;
-    memcpy(&u, &f, sizeof(u));
-    return (long long)u;
-}
 inline float* at(float* A, long long lda, int r, int c) { return A + (long long)c * lda + r; }
 
 struct PrecInfo {
@@ -56,20 +51,22 @@ PrecInfo prec_info(int prec)
 }
 
 // C -= scale * (A B^T) with optional hi/lo split operands.
+// sa / sb (optional): device max slots of per-panel scaled operands.
 hdbf_status tc_update(hdbf_context* ctx, const PrecInfo& pi, int M, int N, int K, const void* ah,
                       const void* al, long long lda, const void* bh, const void* bl, long long ldb,
-                      float* C, long long ldc, float scale, bool lower)
+                      float* C, long long ldc, float scale, bool lower,
+                      const unsigned* sa = nullptr, const unsigned* sb = nullptr)
 {
     TcOperand a, b;
     a.base = ah;
     a.ld = lda;
     b.base = bh;
     b.ld = ldb;
-    if (!pi.split) return tc_gemm_sub(ctx, pi.fmt, M, N, K, a, b, C, ldc, scale, lower);
+    if (!pi.split) return tc_gemm_sub(ctx, pi.fmt, M, N, K, a, b, C, ldc, scale, lower, sa, sb);
     TcOperand alo = a, blo = b;
     alo.base = al;
     blo.base = bl;
-    return tc_gemm_sub_split(ctx, pi.fmt, M, N, K, a, alo, b, blo, C, ldc, scale, lower);
+    return tc_gemm_sub_split(ctx, pi.fmt, M, N, K, a, alo, b, blo, C, ldc, scale, lower, sa, sb);
 }
 
 __global__ void absmax_kernel(const float* A, long long lda, int rows, int cols, int diag_only,
@@ -168,28 +165,100 @@ hdbf_status absmax_host(hdbf_context* ctx, const float* A, long long lda, int ro
     return HDBF_STATUS_SUCCESS;
 }
 
-// Power-of-two scale putting max|x| * s near 2^8 (FP16 range); 1 for BF16.
-float shadow_scale(int fmt, float maxabs)
-{
-    if (fmt != kFmtF16 || !(maxabs > 0.f) || !std::isfinite(maxabs)) return 1.f;
-    const int e = (int)std::lround(std::log2(256.0 / (double)maxabs));
-    return std::ldexp(1.f, std::max(-60, std::min(60, e)));
-}
-
 // Arena: four n x pad8(b) 16-bit shadows (hi/lo of two operands; the
 // panel-TRSM GEMM uses the lo halves as scratch in every mode), then the
 // FP32 inverse block W (b x pad8(b)) and its hi/lo shadows.
 size_t mixed_base_bytes(int n, int b) { return align_up((size_t)4 * n * pad8(b) * 2, 256); }
+// After W: one max slot (FP32 bits, see panel_scale_exp) per panel for the
+// per-panel scales of the FP16 shadows.
+size_t mixed_slots_offset(int n, int b)
+{
+    const size_t w = align_up((size_t)b * pad8(b) * 4, 256) + 2 * align_up((size_t)b * pad8(b) * 2, 256);
+    return mixed_base_bytes(n, b) + w;
+}
+// Slot region: per-panel scale slots, per-panel fallback flags, then the
+// fallback counter (each panels + 2 words); after it the FP32 copy of the
+// original matrix (n x n) the Cholesky panel fallback recomputes from.
+size_t mixed_slot_words(int n, int b) { return (size_t)n / b + 2; }
+size_t mixed_backup_offset(int n, int b)
+{
+    return mixed_slots_offset(n, b) + align_up(3 * mixed_slot_words(n, b) * sizeof(unsigned), 256);
+}
 size_t mixed_shadow_bytes(int n, int b, bool split)
 {
     (void)split;
-    const size_t w = align_up((size_t)b * pad8(b) * 4, 256) + 2 * align_up((size_t)b * pad8(b) * 2, 256);
-    return mixed_base_bytes(n, b) + w + 1024;
+    return mixed_backup_offset(n, b) + align_up((size_t)n * n * sizeof(float), 256) + 1024;
+}
+
+namespace {
+
+// dst(r, c) = src(r, c) for the lower trapezoid r >= c of a rows x cols block
+// column, when *run_if != 0 (the panel fallback's restore of the originals).
+__global__ void restore_lower_kernel(int rows, int cols, const float* src, long long lds,
+                                     float* dst, long long ldd, const int* run_if)
+{
+    if (*run_if == 0) return;
+    const long long total = (long long)rows * cols;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i / rows), r = (int)(i % rows);
+        if (r >= c) dst[(long long)c * ldd + r] = src[(long long)c * lds + r];
+    }
+}
+
+// A panel whose first attempt failed (*flag != 0): count it; when the FP32
+// retry failed too, its info stands (the retry wrote it).
+__global__ void count_fallback_kernel(const int* flag, unsigned* counter)
+{
+    if (*flag != 0) atomicAdd(counter, 1u);
+}
+
+// First panel: nothing precedes it to recompute, so its failure is final.
+__global__ void promote_info_kernel(const int* flag, int* info)
+{
+    if (*flag != 0 && info) atomicCAS(info, 0, *flag);
+}
+
+}  // namespace
+
+// Panel fallback of the mixed Cholesky: if the diagonal block of panel k
+// (rows k.., psz columns) failed after the low-precision trailing updates
+// (*flag != 0, set by the first attempt), the panel's block column is
+// rebuilt in FP32 from the original matrix A0 -- A(k:n, k:k+psz) =
+// A0(k:n, k:k+psz) - L(k:n, 0:k) L(k:k+psz, 0:k)^T with the FP32 GEMM -- and
+// its diagonal block factored again, writing `info` only if that fails too.
+// Every launch is conditional on *flag (RunIf), so the graph of the
+// factorization does the extra work only for panels that need it.
+hdbf_status potrf_panel_fallback(hdbf_context* ctx, float* A, long long lda, const float* A0,
+                                 long long ld0, int n, int k, int psz, const int* flag,
+                                 int* info, float* W, long long ldw, unsigned* counter)
+{
+    if (k == 0) {
+        promote_info_kernel<<<1, 1, 0, ctx->stream>>>(flag, info);
+        ctx->launches++;
+        return last_cuda(ctx);
+    }
+    const int rows = n - k;
+    RunIf ri(ctx, flag);
+    const long long total = (long long)rows * psz;
+    const int g = (int)std::min<long long>((total + 255) / 256, 8LL * ctx->sm_count);
+    restore_lower_kernel<<<g, 256, 0, ctx->stream>>>(rows, psz, A0 + (long long)k * ld0 + k, ld0,
+                                                       at(A, lda, k, k), lda, flag);
+    ctx->launches++;
+    HDBF_TRY(sgemm_sub(ctx, false, true, psz, psz, k, at(A, lda, k, 0), lda, at(A, lda, k, 0), lda,
+                       at(A, lda, k, k), lda));
+    if (rows > psz)
+        HDBF_TRY(sgemm_sub(ctx, false, false, rows - psz, psz, k, at(A, lda, k + psz, 0), lda,
+                           at(A, lda, k, 0), lda, at(A, lda, k + psz, k), lda));
+    HDBF_TRY(potrf_block(ctx, psz, at(A, lda, k, k), lda, info, k, W, ldw));
+    count_fallback_kernel<<<1, 1, 0, ctx->stream>>>(flag, counter);
+    ctx->launches++;
+    return last_cuda(ctx);
 }
 
 // Right-looking mixed Cholesky (lower) with block b; shadows in `arena`.
 hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
-                             int* info, float s, char* arena)
+                             int* info, char* arena)
 {
     const PrecInfo pi = prec_info(prec);
     if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
@@ -198,17 +267,39 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
     void* hi = arena;
     void* lo = pi.split ? arena + one : nullptr;
     void* scratch_lo = arena + one;
-    const float inv_s2 = 1.f / (s * s);
+    // FP16 shadows carry a per-panel power-of-two scale (FP16's range is
+    // narrow); BF16 has FP32's exponent range and needs none.
+    unsigned* slots = reinterpret_cast<unsigned*>(arena + mixed_slots_offset(n, b));
+    const size_t words = mixed_slot_words(n, b);
+    int* fail_flags = reinterpret_cast<int*>(slots + words);
+    unsigned* fallbacks = slots + 2 * words;
+    const bool scaled = pi.fmt == kFmtF16;
     const PrecInfo tp = trsm_prec(pi);
     const WBlock wb = w_block(arena, n, b);
+    // The panel fallback (BF16 / FP16 modes) rebuilds a failed panel from a
+    // copy of the original matrix.
+    float* A0 = trsm_on_tc(pi) ? reinterpret_cast<float*>(arena + mixed_backup_offset(n, b))
+                               : nullptr;
     if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
+    cudaMemsetAsync(fallbacks, 0, sizeof(unsigned), ctx->stream);
+    if (A0)
+        cudaMemcpy2DAsync(A0, (size_t)n * sizeof(float), A, (size_t)lda * sizeof(float),
+                          (size_t)n * sizeof(float), n, cudaMemcpyDeviceToDevice, ctx->stream);
     for (int k = 0; k < n; k += b) {
+        unsigned* slot = scaled ? slots + k / b : nullptr;
         const int psz = std::min(b, n - k);
         const int tr = n - k - psz;
         float* Akk = at(A, lda, k, k);
         const bool inv_tc = trsm_on_tc(pi) && tr > 0 && psz <= potrf_block_max_n();
-        if (inv_tc) HDBF_TRY(potrf_block(ctx, psz, Akk, lda, info, k, wb.W, wb.ldw));
-        else HDBF_TRY(potrf_diag(ctx, psz, Akk, lda, info, k));
+        if (inv_tc) {
+            int* flag = fail_flags + k / b;
+            cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream);
+            HDBF_TRY(potrf_block(ctx, psz, Akk, lda, flag, k, wb.W, wb.ldw));
+            HDBF_TRY(potrf_panel_fallback(ctx, A, lda, A0, n, n, k, psz, flag, info, wb.W, wb.ldw,
+                                          fallbacks));
+        } else {
+            HDBF_TRY(potrf_diag(ctx, psz, Akk, lda, info, k));
+        }
         if (tr <= 0) continue;
         float* A21 = at(A, lda, k + psz, k);
         // L21 = A21 L11^{-T} as one tensor-core GEMM with W = L11^{-1} from
@@ -216,9 +307,10 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         // overwritten with the product.
         if (!inv_tc) {
             HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
-            HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, s));
+            if (slot) HDBF_TRY(panel_absmax(ctx, A21, lda, tr, psz, slot));
+            HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, 1.f, slot));
             HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
-                               at(A, lda, k + psz, k + psz), lda, inv_s2, true));
+                               at(A, lda, k + psz, k + psz), lda, 1.f, true, slot, slot));
             continue;
         }
         // W = L11^{-1} came with the diagonal factorization; the GEMM's B
@@ -230,16 +322,17 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         HDBF_TRY(zero_block(ctx, A21, lda, tr, psz));
         HDBF_TRY(tc_update(ctx, tp, tr, psz, psz, hi, scratch_lo, lds, wb.wh, wb.wl, wb.ldws, A21,
                            lda, -1.f, false));
-        HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, s));
+        if (slot) HDBF_TRY(panel_absmax(ctx, A21, lda, tr, psz, slot));
+        HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, 1.f, slot));
         HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
-                           at(A, lda, k + psz, k + psz), lda, inv_s2, true));
+                           at(A, lda, k + psz, k + psz), lda, 1.f, true, slot, slot));
     }
     return last_cuda(ctx);
 }
 
 // Right-looking mixed LU with partial pivoting and block b.
 hdbf_status getrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
-                             int* ipiv, int* info, float sL, float sU, char* arena)
+                             int* ipiv, int* info, char* arena)
 {
     const PrecInfo pi = prec_info(prec);
     if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
@@ -254,9 +347,13 @@ hdbf_status getrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
     void* scratch_lo = arena + 3 * one;
     const PrecInfo tp = trsm_prec(pi);
     const WBlock wb = w_block(arena, n, b);
-    const float inv_s = 1.f / (sL * sU);
+    // |L| <= 1 under partial pivoting: L's shadow is unscaled; U's FP16 shadow
+    // carries a per-panel power-of-two scale.
+    unsigned* slots = reinterpret_cast<unsigned*>(arena + mixed_slots_offset(n, b));
+    const bool scaled = pi.fmt == kFmtF16;
     if (info) cudaMemsetAsync(info, 0, sizeof(int), ctx->stream);
     for (int p = 0; p < n; p += b) {
+        unsigned* slot = scaled ? slots + p / b : nullptr;
         const int psz = std::min(b, n - p);
         const int next = p + psz;
         const int tr = n - next;
@@ -289,10 +386,12 @@ hdbf_status getrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
             HDBF_TRY(trsm_llu(ctx, psz, tr, at(A, lda, p, p), lda, A12, lda));
         }
         HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, at(A, lda, next, p), lda, hL, lL, lds,
-                                     sL));
-        HDBF_TRY(convert_direct16(ctx, pi.fmt, psz, tr, at(A, lda, p, next), lda, hU, lU, lds, sU));
+                                     1.f));
+        if (slot) HDBF_TRY(panel_absmax(ctx, at(A, lda, p, next), lda, psz, tr, slot));
+        HDBF_TRY(convert_direct16(ctx, pi.fmt, psz, tr, at(A, lda, p, next), lda, hU, lU, lds, 1.f,
+                                  slot));
         HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hL, lL, lds, hU, lU, lds, at(A, lda, next, next),
-                           lda, inv_s, false));
+                           lda, 1.f, false, nullptr, slot));
     }
     return last_cuda(ctx);
 }
@@ -307,15 +406,16 @@ hdbf_status potrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, in
     if (b <= 0) b = 512;
     b = std::min(b, n);
     HDBF_TRY(ensure_ws(ctx, n));
-    float maxdiag = 1.f;
-    if (pi.fmt == kFmtF16) HDBF_TRY(absmax_host(ctx, A, lda, n, n, true, &maxdiag));
-    const float s = shadow_scale(pi.fmt, std::sqrt(maxdiag));  // |L| <= sqrt(max a_ii)
     hdbf_status st;
     char* arena = static_cast<char*>(mixed_arena(ctx, mixed_shadow_bytes(n, b, pi.split), &st));
     if (!arena) return st;
+    ctx->mixed_fallbacks =
+        trsm_on_tc(pi) ? reinterpret_cast<unsigned*>(arena + mixed_slots_offset(n, b)) +
+                             2 * mixed_slot_words(n, b)
+                       : nullptr;
     const std::vector<long long> key = {30, prec, (long long)A, lda, n, b, (long long)info,
-                                        fbits(s), (long long)arena};
-    return run_graph(ctx, key, [&] { return potrf_mixed_body(ctx, prec, A, lda, n, b, info, s, arena); });
+                                        (long long)arena};
+    return run_graph(ctx, key, [&] { return potrf_mixed_body(ctx, prec, A, lda, n, b, info, arena); });
 }
 
 hdbf_status getrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
@@ -328,18 +428,13 @@ hdbf_status getrf_mixed(hdbf_context* ctx, int prec, float* A, long long lda, in
     if (b <= 0) b = 512;
     b = std::min(b, n);
     HDBF_TRY(ensure_ws(ctx, n));
-    float maxa = 1.f;
-    if (pi.fmt == kFmtF16) HDBF_TRY(absmax_host(ctx, A, lda, n, n, false, &maxa));
-    const float sL = 1.f;  // |L| <= 1 under partial pivoting
-    const float sU = shadow_scale(pi.fmt, 8.f * maxa);  // headroom for element growth
     hdbf_status st;
     char* arena = static_cast<char*>(mixed_arena(ctx, mixed_shadow_bytes(n, b, pi.split), &st));
     if (!arena) return st;
     const std::vector<long long> key = {31, prec, (long long)A, lda, n, b, (long long)ipiv,
-                                        (long long)info, fbits(sU),
-                                        (long long)arena};
+                                        (long long)info, (long long)arena};
     return run_graph(ctx, key, [&] {
-        return getrf_mixed_body(ctx, prec, A, lda, n, b, ipiv, info, sL, sU, arena);
+        return getrf_mixed_body(ctx, prec, A, lda, n, b, ipiv, info, arena);
     });
 }
 
@@ -354,6 +449,22 @@ hdbf_status hdbf_spotrf_mixed(hdbf_handle h, hdbf_precision prec, float* A, int 
 {
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
     return h->last_status = potrf_mixed(h, (int)prec, A, lda, n, nb, info);
+}
+
+hdbf_status hdbf_mixed_fallback_panels(hdbf_handle h, int* count)
+{
+    if (!h || !count) return h ? HDBF_STATUS_INVALID_VALUE : HDBF_STATUS_INVALID_HANDLE;
+    *count = 0;
+    if (!h->mixed_fallbacks) return HDBF_STATUS_SUCCESS;
+    unsigned v = 0;
+    if (cudaMemcpyAsync(&v, h->mixed_fallbacks, sizeof(v), cudaMemcpyDeviceToHost, h->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    *count = (int)v;
+    return HDBF_STATUS_SUCCESS;
 }
 
 hdbf_status hdbf_sgetrf_mixed(hdbf_handle h, hdbf_precision prec, float* A, int lda, int n, int nb,

@@ -45,6 +45,7 @@ struct Sync {
     int* err;
     unsigned G;
     unsigned count;  // barriers passed by this CTA
+    unsigned limit;  // poll limit (the handle's, spin_limit_of)
 };
 
 // Grid barrier: arrive (counter += 1 per CTA), wait until all G CTAs of this
@@ -60,7 +61,7 @@ __device__ void grid_barrier(Sync& s)
         unsigned polls = 0;
         while (ld_acquire_u32(s.ctr) < target) {
             if (*reinterpret_cast<volatile int*>(s.abort_flag)) break;
-            if (++polls > kSpinLimit) {
+            if (++polls > s.limit) {
                 atomicExch(s.err, kErrTimeout);
                 atomicExch(s.abort_flag, 1);
                 break;
@@ -196,7 +197,7 @@ __device__ void tri_inv_tile(const float* L, long long ld, int nb, float* Ls /*6
 __global__ void __launch_bounds__(kThreads, 1)
 potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, float* W,
                    long long ldw, float* dinv, float* Tsc, unsigned* ctr, int* fail,
-                   int* abort_flag, int* err)
+                   int* abort_flag, int* err, const int* run_if)
 {
     __shared__ __align__(16) float As[kT * kLdS];
     __shared__ __align__(16) float Bs[kT * kLdS];
@@ -207,11 +208,15 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
     const int cta = blockIdx.x;
     const unsigned G = gridDim.x;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    Sync sy{ctr, fail, abort_flag, err, G, 0u};
+    Sync sy{ctr, fail, abort_flag, err, G, 0u, spin_limit_of(err)};
     auto tile = [&](int i, int j) { return A + (long long)(j * kT) * lda + i * kT; };
     auto ext = [&](int i) { return min(kT, n - i * kT); };
 
-    if (tid == 0) s_flag = (info && *reinterpret_cast<volatile int*>(info) != 0) ? 1 : 0;
+    if (tid == 0)
+        s_flag = ((info && *reinterpret_cast<volatile int*>(info) != 0) ||
+                  (run_if && *reinterpret_cast<const volatile int*>(run_if) == 0))
+                     ? 1
+                     : 0;
     __syncthreads();
     const bool skip = s_flag != 0;  // same value in every CTA: read before any write
     grid_barrier(sy);
@@ -410,8 +415,9 @@ hdbf_status potrf_block(hdbf_context* ctx, int n, float* A, long long lda, int* 
     float* Tsc = ws_skinny(ctx);  // n x n scratch (leading dimension ldw) for the inverse
     const double flops = (double)n * n * n / 3.0 + (W ? (double)n * n * n / 3.0 : 0.0);
     ProfScope prof(ctx, kClsPotrfBlock, flops, 8.0 * n * n, n, n, n);
+    const int* run_if = ctx->run_if;
     void* args[] = {&n, &A, &lda, &info, &info_base, &W, &ldw, &dinv, &Tsc, &ctr, &fail,
-                    &abort_flag, &err};
+                    &abort_flag, &err, &run_if};
     const cudaError_t e = cudaLaunchCooperativeKernel((const void*)potrf_block_kernel, dim3(G),
                                                       dim3(kThreads), args, 0, ctx->stream);
     ctx->launches++;

@@ -1,3 +1,4 @@
+#include <algorithm>
 // Handle, stream pool, workspace arena and status plumbing (host C++).
 #include <cstdio>
 #include <cstdlib>
@@ -209,7 +210,7 @@ ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes, int
     // (a plain record would only express a dependency).
     cudaEventRecordWithFlags(a, ctx->stream, ctx->capturing ? cudaEventRecordExternal : 0);
     idx_ = static_cast<int>(ctx->prof.size());
-    ctx->prof.push_back(ProfRec{cls, a, b, flops, bytes, m, n, k});
+    ctx->prof.push_back(ProfRec{cls, a, b, flops, bytes, m, n, k, ctx->stage, ctx->stage_call});
 }
 
 ProfScope::~ProfScope()
@@ -485,6 +486,8 @@ hdbf_status hdbf_check_device_errors(hdbf_handle h)
         if (h->ws) cudaMemset(h->ws, 0, h->ws_bytes);  // exchange words with the counters
         epoch += 2;
         cudaMemcpy(h->dev_small + kSmallEpoch, &epoch, sizeof(int), cudaMemcpyHostToDevice);
+        cudaMemcpy(h->dev_small + kSmallSpin, &h->spin_limit, sizeof(unsigned),
+                   cudaMemcpyHostToDevice);
         cudaDeviceSynchronize();
         return err == kErrTimeout ? HDBF_STATUS_TIMEOUT : HDBF_STATUS_INVALID_VALUE;
     }
@@ -564,16 +567,31 @@ hdbf_status hdbf_profile_end(hdbf_handle h, int max_classes, double* ms, double*
     // flops, bytes, m, n, k) for offline analysis.
     const char* csv_path = std::getenv("HDBF_PROFILE_CSV");
     FILE* csv = csv_path ? std::fopen(csv_path, "a") : nullptr;
+    for (int st = 0; st < kNumStages; ++st) {
+        h->stage_ms[st] = 0.0;
+        h->stage_flops[st] = 0.0;
+        h->stage_calls[st] = 0;
+    }
+    std::vector<std::pair<int, unsigned>> calls_seen;
     auto add = [&](const ProfRec& r) {
-        if (r.cls < 0 || r.cls >= max_classes) return;
         float t = 0.f;
         if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) {
             cudaGetLastError();
             return;
         }
+        if (r.stage > 0 && r.stage < kNumStages) {
+            h->stage_ms[r.stage] += t;
+            h->stage_flops[r.stage] += r.flops;
+            const std::pair<int, unsigned> key(r.stage, r.call);
+            if (std::find(calls_seen.begin(), calls_seen.end(), key) == calls_seen.end()) {
+                calls_seen.push_back(key);
+                h->stage_calls[r.stage] += 1;
+            }
+        }
+        if (r.cls < 0 || r.cls >= max_classes) return;
         if (csv)
-            std::fprintf(csv, "%s,%.6f,%.6g,%.6g,%d,%d,%d\n", hdbf_profile_class_name(r.cls), t,
-                         r.flops, r.bytes, r.m, r.n, r.k);
+            std::fprintf(csv, "%s,%.6f,%.6g,%.6g,%d,%d,%d,%s\n", hdbf_profile_class_name(r.cls), t,
+                         r.flops, r.bytes, r.m, r.n, r.k, hdbf_profile_stage_name(r.stage));
         if (ms) ms[r.cls] += t;
         if (flops) flops[r.cls] += r.flops;
         if (bytes) bytes[r.cls] += r.bytes;
@@ -614,6 +632,30 @@ const char* hdbf_profile_class_name(int cls)
 
 int hdbf_profile_num_classes(void) { return kNumClasses; }
 
+const char* hdbf_profile_stage_name(int stage)
+{
+    static const char* names[kNumStages] = {
+        "none", "POTRF", "TRSM", "Inner GEMM", "Outer SYRK", "Outer GEMM", "Panel GETRF",
+        "Pivot propagation", "Inner pivot batch", "Inner TRSM", "Outer pivot batch",
+        "Outer TRSM block", "Outer TRSM GEMM", "Outer TRSM direct"};
+    return (stage >= 0 && stage < kNumStages) ? names[stage] : "unknown";
+}
+
+int hdbf_profile_num_stages(void) { return kNumStages; }
+
+hdbf_status hdbf_profile_stages(hdbf_handle h, int max_stages, double* ms, double* flops,
+                                int* calls)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    for (int st = 0; st < max_stages; ++st) {
+        const bool in = st < kNumStages;
+        if (ms) ms[st] = in ? h->stage_ms[st] : 0.0;
+        if (flops) flops[st] = in ? h->stage_flops[st] : 0.0;
+        if (calls) calls[st] = in ? h->stage_calls[st] : 0;
+    }
+    return HDBF_STATUS_SUCCESS;
+}
+
 hdbf_status hdbf_set_panel_kernel(hdbf_handle h, int mode)
 {
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
@@ -628,6 +670,19 @@ hdbf_status hdbf_set_lookahead(hdbf_handle h, int enabled)
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
     if ((enabled != 0) != (h->lookahead != 0)) graph_cache_clear(h);
     h->lookahead = enabled != 0;
+    return HDBF_STATUS_SUCCESS;
+}
+
+hdbf_status hdbf_set_wait_limit(hdbf_handle h, unsigned int polls)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(h->dev_small + kSmallSpin, &polls, sizeof(unsigned), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return HDBF_STATUS_CUDA_ERROR;
+    }
+    h->spin_limit = polls;
     return HDBF_STATUS_SUCCESS;
 }
 

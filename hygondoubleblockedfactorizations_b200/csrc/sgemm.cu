@@ -45,8 +45,9 @@ template <int MODE, bool VEC, bool TRI>
 __global__ void __launch_bounds__(NTHR, 2)
 sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda,
                  const float* __restrict__ B, long long ldb, float* __restrict__ C,
-                 long long ldc, int tiles_m)
+                 long long ldc, int tiles_m, const int* __restrict__ run_if)
 {
+    if (run_if && *run_if == 0) return;  // conditional launch (RunIf) not taken
     constexpr bool AT = MODE == kTN;  // A read k-contiguous (transposed load)
     constexpr bool BT = MODE != kNT;  // B read k-contiguous (transposed load)
     const int tm = blockIdx.x % tiles_m;
@@ -208,13 +209,13 @@ inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 
 template <int MODE, bool VEC, bool TRI>
 void launch_sub(cudaStream_t s, int M, int N, int K, const float* A, long long lda,
-                const float* B, long long ldb, float* C, long long ldc)
+                const float* B, long long ldb, float* C, long long ldc, const int* run_if)
 {
     const int tiles_m = (M + BM - 1) / BM;
     const int tiles_n = (N + BN - 1) / BN;
     const long long grid = (long long)tiles_m * tiles_n;
     sgemm_sub_kernel<MODE, VEC, TRI><<<(unsigned)grid, NTHR, 0, s>>>(M, N, K, A, lda, B, ldb,
-                                                                    C, ldc, tiles_m);
+                                                                    C, ldc, tiles_m, run_if);
 }
 
 hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, int N, int K,
@@ -224,7 +225,7 @@ hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, in
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
     if (!A || !B || !C) return HDBF_STATUS_INVALID_VALUE;
     if (lower_only && mode != kNT) return HDBF_STATUS_INVALID_VALUE;
-    if (!lower_only && !ctx->no_skinny && N <= 32 && M >= 4 * N && M >= 256)
+    if (!lower_only && !ctx->no_skinny && !ctx->run_if && N <= 32 && M >= 4 * N && M >= 256)
         return sgemm_skinny(ctx, mode == kNT ? 0 : mode == kNN ? 1 : 2, M, N, K, A, lda, B, ldb,
                             C, ldc);
     const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
@@ -232,6 +233,7 @@ hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, in
     const bool vec = aligned16(A) && aligned16(B) && aligned16(C) && (lda % 4 == 0) &&
                      (ldb % 4 == 0) && (ldc % 4 == 0);
     cudaStream_t s = ctx->stream;
+    const int* ri = ctx->run_if;
     double flops = 2.0 * (double)M * N * K;
     if (lower_only) {
         // only entries with row >= col: sum over cols j < min(M,N) of (M - j)
@@ -242,18 +244,18 @@ hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, in
                    N, K);
     if (mode == kNT) {
         if (vec) {
-            if (lower_only) launch_sub<kNT, true, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
-            else launch_sub<kNT, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+            if (lower_only) launch_sub<kNT, true, true>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+            else launch_sub<kNT, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
         } else {
-            if (lower_only) launch_sub<kNT, false, true>(s, M, N, K, A, lda, B, ldb, C, ldc);
-            else launch_sub<kNT, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+            if (lower_only) launch_sub<kNT, false, true>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+            else launch_sub<kNT, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
         }
     } else if (mode == kNN) {
-        if (vec) launch_sub<kNN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
-        else launch_sub<kNN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        if (vec) launch_sub<kNN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+        else launch_sub<kNN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
     } else {
-        if (vec) launch_sub<kTN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
-        else launch_sub<kTN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc);
+        if (vec) launch_sub<kTN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+        else launch_sub<kTN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
     }
     ctx->launches++;
     return last_cuda(ctx);

@@ -121,6 +121,8 @@ struct TcArgs {
     float* C;
     long long ldc;
     float scale;
+    const unsigned* sa_max;  // optional per-panel scale sources (panel_scale_exp)
+    const unsigned* sb_max;
     int tiles_m;
     int lower;
     int fmt;
@@ -250,6 +252,9 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
     asm volatile("tcgen05.fence::after_thread_sync;");
     __syncthreads();
     if (ok && !s_fail && ktiles > 0) {
+        float scale = args.scale;  // undo the operands' per-panel scales
+        if (args.sa_max) scale *= pow2f_exact(-panel_scale_exp(*args.sa_max));
+        if (args.sb_max) scale *= pow2f_exact(-panel_scale_exp(*args.sb_max));
         const uint32_t lane_base = taddr + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
         for (int c0 = 0; c0 < TN; c0 += 32) {
@@ -281,7 +286,7 @@ tc_gemm_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_consta
                     const int col = n0 + c0 + j;
                     if (col < args.N && (!args.lower || row >= col))
                         args.C[(long long)col * args.ldc + row] =
-                            fmaf(-args.scale, __uint_as_float(v[j]), cv[j]);
+                            fmaf(-scale, __uint_as_float(v[j]), cv[j]);
                 }
             }
         }
@@ -345,7 +350,8 @@ void configure_tc_kernels(hdbf_context* ctx)
 namespace {
 hdbf_status tc_launch(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
                       const TcOperand& B, const TcOperand* Alo, const TcOperand* Blo, float* C,
-                      long long ldc, float scale, bool lower_only)
+                      long long ldc, float scale, bool lower_only, const unsigned* sa_max,
+                      const unsigned* sb_max)
 {
     if (M <= 0 || N <= 0 || K <= 0) return HDBF_STATUS_SUCCESS;
     const bool split = Alo && Blo;
@@ -383,6 +389,8 @@ hdbf_status tc_launch(hdbf_context* ctx, int fmt, int M, int N, int K, const TcO
     args.C = C;
     args.ldc = ldc;
     args.scale = scale;
+    args.sa_max = sa_max;
+    args.sb_max = sb_max;
     args.tiles_m = (M + TM - 1) / TM;
     args.lower = lower_only ? 1 : 0;
     args.fmt = fmt;
@@ -412,16 +420,20 @@ hdbf_status tc_launch(hdbf_context* ctx, int fmt, int M, int N, int K, const TcO
 }  // namespace
 
 hdbf_status tc_gemm_sub(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
-                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only)
+                        const TcOperand& B, float* C, long long ldc, float scale, bool lower_only,
+                        const unsigned* sa_max, const unsigned* sb_max)
 {
-    return tc_launch(ctx, fmt, M, N, K, A, B, nullptr, nullptr, C, ldc, scale, lower_only);
+    return tc_launch(ctx, fmt, M, N, K, A, B, nullptr, nullptr, C, ldc, scale, lower_only, sa_max,
+                     sb_max);
 }
 
 hdbf_status tc_gemm_sub_split(hdbf_context* ctx, int fmt, int M, int N, int K, const TcOperand& A,
                               const TcOperand& Alo, const TcOperand& B, const TcOperand& Blo,
-                              float* C, long long ldc, float scale, bool lower_only)
+                              float* C, long long ldc, float scale, bool lower_only,
+                              const unsigned* sa_max, const unsigned* sb_max)
 {
-    return tc_launch(ctx, fmt, M, N, K, A, B, &Alo, &Blo, C, ldc, scale, lower_only);
+    return tc_launch(ctx, fmt, M, N, K, A, B, &Alo, &Blo, C, ldc, scale, lower_only, sa_max,
+                     sb_max);
 }
 
 }  // namespace hdbf

@@ -63,6 +63,17 @@ size_t hdbf_workspace_bytes_for(int n);
  * HDBF_STATUS_TIMEOUT if any kernel gave up, else the CUDA status. */
 hdbf_status hdbf_check_device_errors(hdbf_handle handle);
 
+/* Poll limit of every bounded device-side wait on this handle (the grid-wide
+ * barriers and exchanges of the GETRF panel, diagonal-block Cholesky and
+ * wavefront-solve kernels, FP32 and FP64).  0 restores the default, 2^22 polls
+ * (about half a second with back-off).  A wait that runs out records
+ * HDBF_STATUS_TIMEOUT, which hdbf_check_device_errors returns once (it then
+ * clears the error word and the exchange state, keeping this limit), and the
+ * kernel returns without finishing the factorization.  Takes effect for the
+ * next launch, recorded graphs included; synchronous, not for use during a
+ * stream capture. */
+hdbf_status hdbf_set_wait_limit(hdbf_handle handle, unsigned int polls);
+
 /* Stream pool (replaces `new StreamPool(n)` / `delete pool`). */
 hdbf_status hdbf_stream_pool_create(int num_streams, StreamPool** pool);
 hdbf_status hdbf_stream_pool_destroy(StreamPool* pool);
@@ -120,6 +131,20 @@ hdbf_status hdbf_profile_end(hdbf_handle handle, int max_classes, double* ms, do
                              double* bytes, unsigned long long* launches);
 const char* hdbf_profile_class_name(int cls);
 int hdbf_profile_num_classes(void);
+
+/* Per-stage split of the last hdbf_profile_begin/end interval: for each stage
+ * of the double-blocked drivers (index 1 .. hdbf_profile_num_stages()-1, named
+ * by hdbf_profile_stage_name as the reference's stage profilers name them:
+ * "POTRF", "TRSM", "Inner GEMM", "Outer SYRK", "Outer GEMM", "Panel GETRF",
+ * "Pivot propagation", "Inner pivot batch", "Inner TRSM", "Outer pivot batch",
+ * "Outer TRSM block", "Outer TRSM GEMM", "Outer TRSM direct"), the summed
+ * device time of its launches in ms, their algorithmic flops, and the number
+ * of times the driver entered the stage.  Index 0 collects launches outside
+ * any stage and is not reported. */
+int hdbf_profile_num_stages(void);
+const char* hdbf_profile_stage_name(int stage);
+hdbf_status hdbf_profile_stages(hdbf_handle handle, int max_stages, double* ms, double* flops,
+                                int* calls);
 
 #ifdef __cplusplus
 }

@@ -27,9 +27,18 @@ typedef enum hdbf_precision {
 } hdbf_precision;
 
 /* Right-looking block-nb factorizations with FP32 panels and trailing updates
- * in `prec`; info as the FP32 routines (first failing column, 1-based). */
+ * in `prec`; info as the FP32 routines (first failing column, 1-based).
+ * FP16 shadows carry a power-of-two scale per panel, computed on the device
+ * from the panel's max |x| (no host synchronisation).  Cholesky panel
+ * fallback (BF16 and FP16 modes): when a diagonal block meets a non-positive
+ * pivot after the low-precision trailing updates, that panel's block column
+ * is rebuilt in FP32 from a device copy of the original matrix (FP32 GEMM of
+ * the preceding panels) and factored again; info is set only if the FP32
+ * panel fails too.  hdbf_mixed_fallback_panels reports how many panels of the
+ * handle's last mixed Cholesky took the fallback (synchronises the stream). */
 hdbf_status hdbf_spotrf_mixed(hdbf_handle handle, hdbf_precision prec, float* A, int lda, int n,
                               int nb, int* info);
+hdbf_status hdbf_mixed_fallback_panels(hdbf_handle handle, int* count);
 hdbf_status hdbf_sgetrf_mixed(hdbf_handle handle, hdbf_precision prec, float* A, int lda, int n,
                               int nb, int* ipiv, int* info);
 
@@ -52,6 +61,7 @@ typedef struct hdbf_ir_info {
     double factor_ms;         /* device time of the factorizations */
     double refine_ms;         /* device time of solves + residuals + updates */
     int inner_iterations;     /* GMRES-IR: preconditioned GMRES steps over all outer steps */
+    int fallback_panels;      /* Cholesky panels rebuilt in FP32 by the last factorization */
 } hdbf_ir_info;
 
 /* Solve A X = B (A SPD for posv, general for gesv; A, B, X FP64).  The FP64 A

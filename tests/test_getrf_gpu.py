@@ -356,3 +356,23 @@ def test_panel_exchange_after_narrow_launch(hd, handle, torch_cuda):
             assert getrf_check(LU[:n], G, ipiv) <= BOUND
     finally:
         handle.set_panel_kernel(0)
+
+
+@pytest.mark.parametrize("fn", ["double_blocked_getrf", "double_blocked_getrf_batched_pivot"])
+def test_long_swap_sequences(hd, handle, torch_cuda, fn):
+    """Inner panels of 4608 columns: their swap sequences are longer than the
+    sorted-group composition takes (4096), so the one-thread replay composes
+    them; inside the panel the recursion's halves use the sorted-group
+    kernel.  Pivots follow host sgetrf; residual within the bound."""
+    import ctypes
+    n = 4608 + 77
+    G = oracle.general_uniform(n, 13)
+    kw = {}
+    if fn.endswith("batched_pivot"):
+        ws, keep = make_ws(torch_cuda, n, tile=32)
+        kw = dict(ws=ctypes.byref(ws))
+    _, LU, ipiv, info = run_getrf(hd, handle, torch_cuda, G, fn, outer=4608, inner=4608, **kw)
+    handle.check()
+    assert info == 0 and handle.device_errors() == 0
+    assert_pivots_match(G, ipiv, oracle.lapack_sgetrf(G)[1], "host sgetrf")
+    assert oracle.scaled(oracle.getrf_residual_tiled(LU[:n], G, ipiv), n) <= BOUND
