@@ -11,6 +11,14 @@ counter-based U[-1,1) stream; GETRF: U[-1,1)), runs one warm-up call (which
 also records the call's profiled CUDA graph), then ``reps`` profiled calls, and prints
 one JSON line: total time, TFLOP/s (n^3/3 or 2n^3/3) and, per kernel class,
 launches, milliseconds, share of the device time and TFLOP/s or GB/s.
+``--stage-samples`` adds the reference's stage tables
+(src/getrf/profile_double_blocked_getrf.cpp, src/potrf/profile_double_blocked_potrf.cpp):
+for each of the ``--reps`` profiled calls a ``STAGE_SAMPLE <OP> iteration=<i>``
+table of the driver's stages (Stage | Total(ms) | Calls | Avg(ms) | Share |
+GFLOPS, the layout of include/utils/benchmark/stage_breakdown_profiler.h:91-130),
+then the spread of each stage and of the total over the samples (mean, sample
+standard deviation, relative standard deviation in percent, minimum and
+maximum, as the reference's stage-spread statistics).
 ``--panel`` selects the GETRF panel kernel (0 automatic, 1 grid-wide,
 2 cluster); ``--batched`` runs the FP32 GETRF through
 ``double_blocked_getrf_batched_pivot`` (iterative outer TRSM, as the
@@ -44,6 +52,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--batched", action="store_true")
     ap.add_argument("--lookahead", type=int, default=None)
+    ap.add_argument("--stage-samples", action="store_true")
     a = ap.parse_args(argv)
 
     P = ctypes.c_void_p
@@ -103,6 +112,16 @@ def main(argv=None):
     torch.cuda.synchronize()
     h.profile_end()
     h.check("warm-up")
+    samples = []
+    if a.stage_samples:
+        for it in range(a.reps):
+            h.profile_begin()
+            run()
+            torch.cuda.synchronize()
+            h.profile_end()
+            samples.append(h.profile_stages())
+            print_stage_sample(a.op.upper(), it + 1, samples[-1])
+        print_spread(samples)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     h.profile_begin()
     e0.record()
@@ -123,8 +142,50 @@ def main(argv=None):
     out = {"op": a.op, "precision": a.precision, "n": n, "outer": a.outer, "inner": a.inner,
            "panel": a.panel, "batched": a.batched, "lookahead": a.lookahead, "ms": round(ms, 3), "tflops": round(flops / (ms / 1e3) / 1e12, 3),
            "info": int(info.item()), "device_errors": h.device_errors(), "stages": stages}
+    if samples:
+        out["stage_spread"] = spread(samples)
     print(json.dumps(out), flush=True)
     return out
+
+
+def print_stage_sample(op, iteration, stages, width=110):
+    """One STAGE_SAMPLE table (stage_breakdown_profiler.h:91-130 layout)."""
+    print("=" * width)
+    print(f"STAGE_SAMPLE {op} iteration={iteration}")
+    print("=" * width)
+    print(f"{'Stage':24s} | {'Total(ms)':>12s} | {'Calls':>10s} | {'Avg(ms)':>12s} | "
+          f"{'Share':>10s} | {'GFLOPS':>12s}")
+    print("-" * width)
+    total = sum(v[1] for v in stages.values())
+    for name, (calls, t, fl) in stages.items():
+        share = 100.0 * t / total if total > 0 else 0.0
+        gf = fl / (t / 1e3) / 1e9 if t > 0 else 0.0
+        print(f"{name:24s} | {t:12.3f} | {calls:10d} | {t / max(calls, 1):12.3f} | "
+              f"{share:9.2f}% | {gf:12.2f}")
+    print("=" * width)
+
+
+def spread(samples):
+    """Per stage and for the total: mean, sample SD, RSD %, min, max (ms)."""
+    import statistics
+    names = list(dict.fromkeys(k for smp in samples for k in smp))
+    out = {}
+    for name in names + ["Total"]:
+        vals = [sum(v[1] for v in smp.values()) if name == "Total" else smp.get(name, (0, 0.0, 0))[1]
+                for smp in samples]
+        mean = statistics.mean(vals)
+        sd = statistics.stdev(vals) if len(vals) > 1 else 0.0
+        out[name] = {"mean_ms": round(mean, 4), "sample_sd_ms": round(sd, 4),
+                     "rsd_percent": round(100.0 * sd / mean, 4) if mean > 0 else 0.0,
+                     "min_ms": round(min(vals), 4), "max_ms": round(max(vals), 4)}
+    return out
+
+
+def print_spread(samples):
+    print(f"{'stage':24s},mean_ms,sample_sd_ms,rsd_percent,min_ms,max_ms")
+    for name, st in spread(samples).items():
+        print(f"{name:24s},{st['mean_ms']},{st['sample_sd_ms']},{st['rsd_percent']},"
+              f"{st['min_ms']},{st['max_ms']}")
 
 
 if __name__ == "__main__":
