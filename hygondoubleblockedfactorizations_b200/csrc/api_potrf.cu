@@ -53,9 +53,13 @@ hdbf_status gemm_nt_rows(hdbf_context* ctx, int rows, int cols, int k, const T* 
     if (rows <= 0 || cols <= 0 || k <= 0) return HDBF_STATUS_SUCCESS;
     int r = 0;
     if (diag_first) {
-        const int d = std::min(rows, cols);
-        HDBF_TRY(gemm_sub(ctx, false, true, d, cols, k, A, lda, B, ldb, C, ldc));
-        r = d;
+        // One lower-trapezoid launch covers the diagonal block and the rows
+        // below it (of the first M tile), so the small diagonal block does not
+        // run as a separate, mostly idle launch.  Each entry is the same k-order
+        // sum either way.
+        const int first = std::min(rows, std::max(cols, m_tile > 0 ? m_tile : rows));
+        HDBF_TRY(gemm_sub(ctx, false, true, first, cols, k, A, lda, B, ldb, C, ldc));
+        r = first;
     }
     const int tile = m_tile > 0 ? m_tile : rows;
     for (; r < rows; r += tile) {
@@ -148,6 +152,16 @@ hdbf_status potrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int nb, int b
             const int nsz = std::min(nb, n - next);
             const int below = next + nsz;
             const int tk = (syrk_k_tile > 0 && syrk_k_tile < next) ? syrk_k_tile : next;
+            if (tk == next) {
+                // Unblocked K: the SYRK of the next diagonal block and the
+                // GEMM below it share both operands and K, so one
+                // lower-trapezoid launch does both (same per-entry sums).
+                StageScope sc(ctx, kStOuterGemm);
+                HDBF_TRY(gemm_nt_rows(ctx, n - next, nsz, next, at(A, lda, next, 0), lda,
+                                      at(A, lda, next, 0), lda, at(A, lda, next, next), lda, 0,
+                                      true));
+                continue;
+            }
             {
                 StageScope sc(ctx, kStOuterSyrk);
                 for (int k0 = 0; k0 < next; k0 += tk) {

@@ -628,7 +628,7 @@ getf2_coop64_kernel(int m, int w, double* A, long long lda, int rpc, int* ipiv, 
             unsigned polls = 0;
             while (ld_acquire_u32(reinterpret_cast<const unsigned*>(sq)) != seq) {
                 if (++polls > spin_limit_of(err)) {
-                    atomicExch(err, kErrTimeout);
+                    atomicCAS(err, 0, kErrTimeout);
                     s_abort = 1;
                     break;
                 }

@@ -206,7 +206,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
             unsigned long long wv;
             while (((unsigned)((wv = ld_relaxed_u64(wq)) >> 16) & 0xffffu) != tag) {
                 if (++polls > spin) {
-                    atomicExch(err, kErrTimeout);
+                    atomicCAS(err, 0, kErrTimeout);
                     s_abort = 1;
                     break;
                 }
@@ -254,7 +254,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                 while ((unsigned)(wp >> 32) != want || (unsigned)(wo >> 32) != want ||
                        (fin && ((unsigned)(wl >> 32) != want || (unsigned)(wm >> 32) != want))) {
                     if (++polls > spin) {
-                        atomicExch(err, kErrTimeout);
+                        atomicCAS(err, 0, kErrTimeout);
                         s_abort = 1;
                         break;
                     }
@@ -507,7 +507,7 @@ compose_swaps_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus, int m,
         if (tid == 0) {
             *count = 0;
             if (info) atomicExch(info, -1);
-            atomicExch(err, kErrBadPivot);
+            atomicCAS(err, 0, kErrBadPivot);
         }
         return;
     }
@@ -553,7 +553,7 @@ compose_swaps_serial_kernel(const int* __restrict__ ipiv, int k, int ipiv_minus,
         if (tid == 0) {
             *count = 0;
             if (info) atomicExch(info, -1);
-            atomicExch(err, kErrBadPivot);
+            atomicCAS(err, 0, kErrBadPivot);
         }
         return;
     }
@@ -615,7 +615,7 @@ compose_running_kernel(const int* __restrict__ ipiv, int k0, int k1, int ipiv_mi
         if (tid == 0) {
             *count = 0;
             if (info) atomicExch(info, -1);
-            atomicExch(err, kErrBadPivot);
+            atomicCAS(err, 0, kErrBadPivot);
         }
         return;
     }

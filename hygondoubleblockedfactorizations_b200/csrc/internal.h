@@ -144,7 +144,8 @@ constexpr int kSmallScratch = 24;    // host-read reduction results (absmax etc.
 constexpr int kSmallBlockBar = 32;   // diagonal-block kernel: barrier counter, fail, abort
 constexpr int kSmallInts = 64;
 
-// Device error codes written into dev_small[kSmallErr].
+// Device error codes written into dev_small[kSmallErr]; the first error
+// recorded stays (atomicCAS from 0) until hdbf_check_device_errors reads it.
 constexpr int kErrTimeout = 1;
 constexpr int kErrBadPivot = 2;
 

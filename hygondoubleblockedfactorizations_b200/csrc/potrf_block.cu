@@ -62,7 +62,7 @@ __device__ void grid_barrier(Sync& s)
         while (ld_acquire_u32(s.ctr) < target) {
             if (*reinterpret_cast<volatile int*>(s.abort_flag)) break;
             if (++polls > s.limit) {
-                atomicExch(s.err, kErrTimeout);
+                atomicCAS(s.err, 0, kErrTimeout);
                 atomicExch(s.abort_flag, 1);
                 break;
             }

@@ -82,7 +82,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
         if (clock64() - t0 > kWaitCycles) {
-            atomicExch(err, kErrTimeout);
+            atomicCAS(err, 0, kErrTimeout);
             return false;
         }
     }

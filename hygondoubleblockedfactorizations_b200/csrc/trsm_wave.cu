@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kWT, 2) trsv_wave_kernel(int n, int nrhs, cons
                 while (ld_acquire_u32(flags + j) == 0u) {
                     if (*reinterpret_cast<volatile int*>(abortp)) { s_abort = 1; break; }
                     if (++polls > spin_limit_of(err)) {
-                        atomicExch(err, kErrTimeout);
+                        atomicCAS(err, 0, kErrTimeout);
                         atomicExch(abortp, 1);
                         s_abort = 1;
                         break;

@@ -53,6 +53,9 @@ def main(argv=None):
     ap.add_argument("--batched", action="store_true")
     ap.add_argument("--lookahead", type=int, default=None)
     ap.add_argument("--stage-samples", action="store_true")
+    ap.add_argument("--syrk-k-tile", type=int, default=0,
+                    help="FP32 POTRF: K tile of the outer SYRK (0: the SYRK runs inside the "
+                         "outer GEMM launch)")
     a = ap.parse_args(argv)
 
     P = ctypes.c_void_p
@@ -90,7 +93,7 @@ def main(argv=None):
                  1, 0, P(ipiv.data_ptr()), P(info.data_ptr()))
         elif a.precision == "fp32" and a.op == "potrf":
             call("double_blocked_potrf_kblocked_syrk", h.ptr, P(A.data_ptr()), n, n, a.outer,
-                 a.inner, 0, P(info.data_ptr()))
+                 a.inner, a.syrk_k_tile, P(info.data_ptr()))
         elif a.precision == "fp32" and a.batched:
             call("double_blocked_getrf_batched_pivot", h.ptr, P(A.data_ptr()), n, n, a.outer,
                  a.inner, 1, 0, 0, P(ipiv.data_ptr()), P(info.data_ptr()), ctypes.byref(ws))

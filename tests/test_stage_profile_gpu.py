@@ -9,6 +9,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("argv,want", [
     (["--op", "potrf", "--n", "2048", "--outer", "512", "--inner", "128"],
+     {"POTRF", "TRSM", "Inner GEMM", "Outer GEMM"}),  # SYRK inside the outer GEMM launch
+    (["--op", "potrf", "--n", "2048", "--outer", "512", "--inner", "128", "--syrk-k-tile", "256"],
      {"POTRF", "TRSM", "Inner GEMM", "Outer SYRK", "Outer GEMM"}),
     (["--op", "getrf", "--n", "2048", "--outer", "1024", "--inner", "256", "--batched"],
      {"Panel GETRF", "Inner pivot batch", "Inner TRSM", "Inner GEMM", "Outer pivot batch",
