@@ -1,9 +1,9 @@
 // Allocation-free variant of trsm_right_lower_transpose.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// triangular solve: code that runs while a CUDA graph is being captured,
-// real-time or embedded services whose memory is fixed at start-up, and host
-// libraries that hand out only caller-owned buffers.  The regular entry point
+// triangular solve: real-time or embedded services whose device memory is
+// fixed at start-up, and host libraries that may hand out only caller-owned
+// buffers.  The regular entry point
 // allocates a per-handle workspace (and the handle itself allocates on
 // creation); this one takes a bare stream and keeps its only scratch -- the
 // inverted 64x64 diagonal blocks of L -- in a fixed-size device array that is

@@ -42,7 +42,8 @@ def main(argv=None):
     from .tuner import _matrix
 
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--op", choices=["potrf", "getrf"], default="getrf")
+    ap.add_argument("--op", choices=["potrf", "getrf", "posv", "gesv", "batched"],
+                    default="getrf")
     ap.add_argument("--precision", choices=list(PREC) + ["fp64"], default="fp32")
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--outer", type=int, default=8192)
@@ -53,12 +54,16 @@ def main(argv=None):
     ap.add_argument("--batched", action="store_true")
     ap.add_argument("--lookahead", type=int, default=None)
     ap.add_argument("--stage-samples", action="store_true")
+    ap.add_argument("--trsm-block", type=int, default=0,
+                    help="GETRF --batched: row block of the iterative outer TRSM (0: direct)")
     ap.add_argument("--syrk-k-tile", type=int, default=0,
                     help="FP32 POTRF: K tile of the outer SYRK (0: the SYRK runs inside the "
                          "outer GEMM launch)")
     a = ap.parse_args(argv)
 
     P = ctypes.c_void_p
+    if a.op in ("posv", "gesv", "batched"):
+        return solve_driver(torch, a)
     h = Handle(torch.cuda.current_stream().cuda_stream)
     if a.panel is not None:
         h.set_panel_kernel(a.panel)
@@ -96,7 +101,8 @@ def main(argv=None):
                  a.inner, a.syrk_k_tile, P(info.data_ptr()))
         elif a.precision == "fp32" and a.batched:
             call("double_blocked_getrf_batched_pivot", h.ptr, P(A.data_ptr()), n, n, a.outer,
-                 a.inner, 1, 0, 0, P(ipiv.data_ptr()), P(info.data_ptr()), ctypes.byref(ws))
+                 a.inner, 1, a.trsm_block, 0, P(ipiv.data_ptr()), P(info.data_ptr()),
+                 ctypes.byref(ws))
         elif a.precision == "fp32":
             call("double_blocked_getrf", h.ptr, P(A.data_ptr()), n, n, a.outer, a.inner, 0, 0,
                  P(ipiv.data_ptr()), P(info.data_ptr()))
@@ -125,21 +131,25 @@ def main(argv=None):
             samples.append(h.profile_stages())
             print_stage_sample(a.op.upper(), it + 1, samples[-1])
         print_spread(samples)
+    # wall time of `reps` calls without the profiler, then one profiled call
+    # for the per-class split (a profiled graph replay keeps one replay's times)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    h.profile_begin()
     e0.record()
     for _ in range(a.reps):
         run()
     e1.record()
     torch.cuda.synchronize()
-    prof = h.profile_end()
     ms = e0.elapsed_time(e1) / a.reps
+    h.profile_begin()
+    run()
+    torch.cuda.synchronize()
+    prof = h.profile_end()
     flops = n ** 3 / 3.0 if a.op == "potrf" else 2.0 * n ** 3 / 3.0
-    dev_ms = sum(v[1] for v in prof.values()) / a.reps
+    dev_ms = sum(v[1] for v in prof.values())
     stages = {}
     for k, (nl, t, fl, by) in sorted(prof.items(), key=lambda kv: -kv[1][1]):
-        stages[k] = {"launches": nl // a.reps, "ms": round(t / a.reps, 3),
-                     "share": round(t / a.reps / dev_ms, 4) if dev_ms else None,
+        stages[k] = {"launches": nl, "ms": round(t, 3),
+                     "share": round(t / dev_ms, 4) if dev_ms else None,
                      "tflops": round(fl / (t / 1e3) / 1e12, 3) if fl and t else None,
                      "gbs": round(by / (t / 1e3) / 1e9, 1) if by and t else None}
     out = {"op": a.op, "precision": a.precision, "n": n, "outer": a.outer, "inner": a.inner,
@@ -148,6 +158,66 @@ def main(argv=None):
     if samples:
         out["stage_spread"] = spread(samples)
     print(json.dumps(out), flush=True)
+    return out
+
+
+def solve_driver(torch, a):
+    """--op posv / gesv: one mixed-precision (or FP32) factorization plus FP64
+    classical refinement (hdbf_dposv_mixed / hdbf_dgesv_mixed, nrhs 16) on an
+    SPD / general matrix with eigen- / singular values log-spaced in [1, 1e2];
+    --op batched: the uneven batched factor-and-solve launch on a batch of
+    --n systems (SPD n ~ U[16, 512] and general n ~ U[32, 768], half each).
+    Runs --reps calls after one warm-up and prints the per-class profile."""
+    import ctypes
+
+    from . import PREC, Handle, IrInfo, call
+    from . import batch as bm
+    P = ctypes.c_void_p
+    h = Handle(torch.cuda.current_stream().cuda_stream)
+    if a.op == "batched":
+        ops, ns = bm.config3_sizes(n_spd=a.n // 2, n_gen=a.n - a.n // 2)
+        b = bm.DeviceBatch(torch, ops, ns)
+        bm.fill_batch(torch, h, b, 3)
+
+        def run():
+            bm.restore(b)
+            assert b.run(h, 2) == 0
+    else:
+        n, nrhs = a.n, 16
+        g = torch.Generator(device="cuda")
+        g.manual_seed(a.seed)
+        Q, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g))
+        lam = torch.logspace(0.0, 2.0, n, dtype=torch.float64, device="cuda")
+        if a.op == "posv":
+            A = (Q * lam) @ Q.t()
+            A = 0.5 * (A + A.t())
+        else:
+            V, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device="cuda",
+                                               generator=g))
+            A = (Q * lam) @ V.t()
+        A = A.t().contiguous()
+        B = torch.randn(nrhs, n, dtype=torch.float64, device="cuda", generator=g)
+        X = torch.zeros_like(B)
+        fn = "hdbf_dposv_mixed" if a.op == "posv" else "hdbf_dgesv_mixed"
+
+        def run():
+            info = IrInfo()
+            st = call(fn, h.ptr, PREC[a.precision], 0, P(A.data_ptr()), n, n, nrhs,
+                      P(B.data_ptr()), n, P(X.data_ptr()), n, ctypes.c_double(1e-13), 30,
+                      ctypes.byref(info))
+            assert st == 0 and info.converged == 1, (st, info.backward_error)
+    for _ in range(max(1, a.reps)):  # warm-up (records the graphs)
+        run()
+    torch.cuda.synchronize()
+    h.profile_begin()
+    run()
+    torch.cuda.synchronize()
+    prof = h.profile_end()
+    out = {"op": a.op, "precision": a.precision, "n": a.n,
+           "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)}
+                       for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+    print(json.dumps(out), flush=True)
+    h.close()
     return out
 
 

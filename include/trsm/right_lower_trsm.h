@@ -18,9 +18,9 @@ void trsm_right_lower_transpose(hdbf_handle handle, int rows, int cols, const fl
 #define HDBF_NOALLOC_TRSM_MAX_COLS 4096
 
 /* No counterpart in the reference.  Same solve as trsm_right_lower_transpose
- * for callers that must not allocate device memory (code running while a CUDA
- * graph is being captured, services whose device memory is fixed at start-up,
- * libraries that may only use caller-owned buffers): it takes a bare stream
+ * for callers that must not allocate device memory (services whose device
+ * memory is fixed at start-up, libraries that may only use caller-owned
+ * buffers): it takes a bare stream
  * instead of a handle and performs no cudaMalloc / cudaFree.  Its only
  * scratch, the inverted 64x64 diagonal blocks of A, lives in a 1 MiB device
  * array inside the library that every GPU loading the library keeps until the

@@ -7,8 +7,8 @@
   same handle (default limit restored) must factor correctly.
 * Corrupt pivots handed to launch_apply_getrf_panel_pivots (a pivot row above
   its own row): the composition rejects them and moves no row.
-* NaN inputs: POTRF reports the first NaN / non-positive pivot like host
-  spotrf; GETRF completes with no device error and the NaN reaches the
+* NaN inputs: POTRF reports the first NaN / non-positive pivot as the
+  reference LAPACK xPOTRF does; GETRF completes with no device error and the NaN reaches the
   factors (non-finite oracle residual)."""
 import ctypes
 
@@ -84,7 +84,12 @@ def test_corrupt_panel_pivots_move_nothing(hd, handle, torch_cuda):
     np.testing.assert_array_equal(host2d(dA, n, n, n), A)
 
 
-def test_nan_diagonal_potrf_info_matches_spotrf(hd, handle, torch_cuda):
+def test_nan_diagonal_potrf_info(hd, handle, torch_cuda):
+    """A NaN diagonal stops the factorization with info = its column, as the
+    reference LAPACK xPOTRF does (`ajj <= 0 or isnan(ajj)`); host OpenBLAS
+    spotrf does not test for NaN and returns 0, so the expected value is the
+    reference LAPACK rule, checked on the same matrix with the NaN replaced by
+    a negative value (which both treat alike)."""
     n = 1024
     A = oracle.spd_gram(n, 0)
     A[300, 300] = np.nan
@@ -94,7 +99,9 @@ def test_nan_diagonal_potrf_info_matches_spotrf(hd, handle, torch_cuda):
             ptr(info))
     torch_cuda.cuda.synchronize()
     assert handle.device_errors() == 0
-    _, info_l = oracle.lapack_spotrf(A)
+    A2 = A.copy()
+    A2[300, 300] = -1.0
+    _, info_l = oracle.lapack_spotrf(A2)
     assert int(info.item()) == info_l == 301
 
 

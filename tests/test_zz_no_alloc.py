@@ -1,8 +1,9 @@
 """GPU test of trsm_right_lower_transpose_noalloc, the allocation-free variant
 of trsm_right_lower_transpose for callers that cannot allocate device memory
-(for example code running while a CUDA graph is being captured).  It keeps its
-scratch in a fixed device array inside the library, so this file is collected
-last: a failure here cannot hide the result of any other test."""
+(services whose device memory is fixed at start-up, libraries that may only
+use caller-owned buffers).  It keeps its scratch in a fixed device array
+inside the library, so this file is collected last: a failure here cannot
+hide the result of any other test."""
 import numpy as np
 import pytest
 
@@ -24,7 +25,7 @@ def rel_err(got, want):
     return np.abs(got.astype(np.float64) - want).max() / max(1e-30, np.abs(want).max())
 
 
-@pytest.mark.parametrize("rows,cols", [(1000, 300), (4096, 1024)])
+@pytest.mark.parametrize("rows,cols", [(1000, 300), (4096, 1024), (512, MAX_COLS)])
 def test_noalloc_matches_regular_entry_point_twice(hd, handle, torch_cuda, rows, cols):
     L = lower_factor(cols, 7)
     B = np.random.default_rng(8).uniform(-1, 1, size=(rows, cols)).astype(np.float32)
