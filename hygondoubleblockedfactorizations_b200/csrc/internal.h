@@ -243,8 +243,12 @@ void* mixed_arena(hdbf_context* ctx, size_t bytes, hdbf_status* st);
 //   skinny  split-K partial sums of the skinny GEMM, 256*n floats
 //   wave  wavefront-solve row-major x copy (32 columns) and its flags
 struct WsLayout {
-    size_t coop, inv, perm, coop64, src, tgt, gperm, temp, skinny, wave, total;
+    size_t coop, inv, perm, coop64, src, tgt, gperm, temp, skinny, wave, split, total;
 };
+// Split-K partial sums of under-filled FP32 GEMM launches: two halves of
+// kSplitFloats each, one for the handle's stream and one for its look-ahead
+// stream, so concurrent GEMMs on the two never share scratch.
+constexpr size_t kSplitFloats = (size_t)5 << 20;
 WsLayout ws_layout(int n);
 // Guarantee the layout for order n (grows the arena outside stream capture).
 hdbf_status ensure_ws(hdbf_context* ctx, int n);
@@ -257,6 +261,8 @@ int* ws_tgt(hdbf_context* ctx);
 int* ws_gperm(hdbf_context* ctx);
 float* ws_temp(hdbf_context* ctx);
 float* ws_skinny(hdbf_context* ctx);
+// Split-K scratch half for GEMMs enqueued on ctx->stream.
+float* ws_split(hdbf_context* ctx);
 float* ws_wave(hdbf_context* ctx);
 
 hdbf_status last_cuda(hdbf_context* ctx);

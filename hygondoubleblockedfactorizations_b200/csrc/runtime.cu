@@ -105,6 +105,8 @@ WsLayout ws_layout(int n)
     off += align_up(skinny_partial_floats(n) * sizeof(float), 256);
     L.wave = off;
     off += wave_scratch_bytes(n);
+    L.split = off;
+    off += align_up(2 * kSplitFloats * sizeof(float), 256);
     L.total = off;
     return L;
 }
@@ -193,6 +195,12 @@ float* ws_wave(hdbf_context* ctx)
 float* ws_skinny(hdbf_context* ctx)
 {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).skinny);
+}
+float* ws_split(hdbf_context* ctx)
+{
+    float* base =
+        reinterpret_cast<float*>(static_cast<char*>(ctx->ws) + ws_layout(ctx->ws_n).split);
+    return (ctx->la_stream && ctx->stream == ctx->la_stream) ? base + kSplitFloats : base;
 }
 
 ProfScope::ProfScope(hdbf_context* ctx, int cls, double flops, double bytes, int m, int n,

@@ -11,6 +11,8 @@
 // from a register prefetch of the next K-slab, one __syncthreads per slab.
 // Two CTAs per SM (<= 128 registers per thread).  Every product is an IEEE
 // FP32 FFMA; accumulation runs in k order from zero, then C - acc.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace hdbf {
@@ -41,17 +43,31 @@ __device__ __forceinline__ float4 load_col4(const float* p, int row, int rows_va
     return v;
 }
 
-template <int MODE, bool VEC, bool TRI>
+template <int MODE, bool VEC, bool TRI, bool SPLIT>
 __global__ void __launch_bounds__(NTHR, 2)
 sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda,
                  const float* __restrict__ B, long long ldb, float* __restrict__ C,
-                 long long ldc, int tiles_m, const int* __restrict__ run_if)
+                 long long ldc, int tiles_m, const int* __restrict__ run_if,
+                 float* __restrict__ part, int kc, int tiles)
 {
     if (run_if && *run_if == 0) return;  // conditional launch (RunIf) not taken
     constexpr bool AT = MODE == kTN;  // A read k-contiguous (transposed load)
     constexpr bool BT = MODE != kNT;  // B read k-contiguous (transposed load)
-    const int tm = blockIdx.x % tiles_m;
-    const int tn = blockIdx.x / tiles_m;
+    // Split K (part != nullptr): CTA blockIdx.x handles K chunk s of tile
+    // blockIdx.x - s * tiles and stores its partial product, from zero, in
+    // part[s] (M x N, leading dimension M); split_reduce_kernel applies them.
+    int bid = blockIdx.x;
+    int split = 0;
+    if (SPLIT) {
+        split = bid / tiles;
+        bid -= split * tiles;
+        const int k0 = split * kc;
+        K = min(kc, K - k0);
+        A += AT ? (long long)k0 : (long long)k0 * lda;
+        B += BT ? (long long)k0 : (long long)k0 * ldb;
+    }
+    const int tm = bid % tiles_m;
+    const int tn = bid / tiles_m;
     const int m0 = tm * BM;
     const int n0 = tn * BN;
     if (TRI && m0 + BM <= n0) return;  // tile strictly above the diagonal
@@ -123,21 +139,7 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
 
-    float4 ra = fetch_a(0);
-    float4 rb = fetch_b(0);
-    stash(0, ra, rb);
-    __syncthreads();
-
-    const int ktiles = (K + BK - 1) / BK;
-    int buf = 0;
-    for (int kt = 0; kt < ktiles; ++kt) {
-        const bool more = kt + 1 < ktiles;
-        if (more) {
-            a_ptr += a_step;
-            b_ptr += b_step;
-            ra = fetch_a((kt + 1) * BK);
-            rb = fetch_b((kt + 1) * BK);
-        }
+    auto slab = [&](int buf) {
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
             const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
@@ -151,15 +153,79 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
 #pragma unroll
                 for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
         }
-        if (more) stash(buf ^ 1, ra, rb);
+    };
+
+    const int ktiles = (K + BK - 1) / BK;
+    // Interior tiles (the bulk of a large update): every operand quad is in
+    // range, so the slab loads carry no bounds tests -- this kernel is
+    // issue-bound, and the tests cost a tenth of its rate.
+    const bool interior = VEC && m0 + BM <= M && n0 + BN <= N && (K % BK) == 0;
+    if (interior) {
+        float4 ra = __ldg(reinterpret_cast<const float4*>(a_ptr));
+        float4 rb = __ldg(reinterpret_cast<const float4*>(b_ptr));
+        stash(0, ra, rb);
         __syncthreads();
-        buf ^= 1;
+        int buf = 0;
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const bool more = kt + 1 < ktiles;
+            if (more) {
+                a_ptr += a_step;
+                b_ptr += b_step;
+                ra = __ldg(reinterpret_cast<const float4*>(a_ptr));
+                rb = __ldg(reinterpret_cast<const float4*>(b_ptr));
+            }
+            slab(buf);
+            if (more) stash(buf ^ 1, ra, rb);
+            __syncthreads();
+            buf ^= 1;
+        }
+    } else {
+        float4 ra = fetch_a(0);
+        float4 rb = fetch_b(0);
+        stash(0, ra, rb);
+        __syncthreads();
+        int buf = 0;
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const bool more = kt + 1 < ktiles;
+            if (more) {
+                a_ptr += a_step;
+                b_ptr += b_step;
+                ra = fetch_a((kt + 1) * BK);
+                rb = fetch_b((kt + 1) * BK);
+            }
+            slab(buf);
+            if (more) stash(buf ^ 1, ra, rb);
+            __syncthreads();
+            buf ^= 1;
+        }
     }
 
-    // Epilogue: C -= acc.  Full interior tiles read all 16 C quads before
-    // writing any (independent loads in flight together).
     const bool full_rows = (m0 + BM <= M);
     const bool full_cols = (n0 + BN <= N);
+    if (SPLIT) {  // split K: store the partial product
+        float* P = part + (long long)split * M * N;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+            if (col >= N) continue;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = m0 + h * 64 + ty * 4;
+                float* pp = P + (long long)col * M + row;
+                if (full_rows && (M & 3) == 0) {
+                    *reinterpret_cast<float4*>(pp) = make_float4(
+                        acc[h * 4 + 0][j], acc[h * 4 + 1][j], acc[h * 4 + 2][j], acc[h * 4 + 3][j]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (row + i < M) pp[i] = acc[h * 4 + i][j];
+                }
+            }
+        }
+        return;
+    }
+    // Epilogue: C -= acc.  Full interior tiles read all 16 C quads before
+    // writing any (independent loads in flight together).
     const bool below_diag = !TRI || (m0 >= n0 + BN);
     if (VEC && full_rows && full_cols && below_diag) {
         float4 cq[8][2];
@@ -205,17 +271,63 @@ sgemm_sub_kernel(int M, int N, int K, const float* __restrict__ A, long long lda
     }
 }
 
+// C -= sum over s of part[s] (in s order), lower triangle only when TRI.
+template <bool TRI>
+__global__ void split_reduce_kernel(int M, int N, int S, const float* __restrict__ part,
+                                    float* __restrict__ C, long long ldc)
+{
+    const long long total = (long long)M * N;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int col = (int)(e / M), row = (int)(e - (long long)col * M);
+        if (TRI && row < col) continue;
+        float acc = part[e];
+        for (int s = 1; s < S; ++s) acc += part[(long long)s * total + e];
+        float* c = C + (long long)col * ldc + row;
+        *c -= acc;
+    }
+}
+
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 template <int MODE, bool VEC, bool TRI>
 void launch_sub(cudaStream_t s, int M, int N, int K, const float* A, long long lda,
-                const float* B, long long ldb, float* C, long long ldc, const int* run_if)
+                const float* B, long long ldb, float* C, long long ldc, const int* run_if,
+                float* part = nullptr, int splits = 1, int kc = 0)
 {
     const int tiles_m = (M + BM - 1) / BM;
     const int tiles_n = (N + BN - 1) / BN;
-    const long long grid = (long long)tiles_m * tiles_n;
-    sgemm_sub_kernel<MODE, VEC, TRI><<<(unsigned)grid, NTHR, 0, s>>>(M, N, K, A, lda, B, ldb,
-                                                                    C, ldc, tiles_m, run_if);
+    const long long tiles = (long long)tiles_m * tiles_n;
+    if (!part) {
+        sgemm_sub_kernel<MODE, VEC, TRI, false><<<(unsigned)tiles, NTHR, 0, s>>>(
+            M, N, K, A, lda, B, ldb, C, ldc, tiles_m, run_if, nullptr, 0, (int)tiles);
+    } else {
+        sgemm_sub_kernel<MODE, VEC, TRI, true><<<(unsigned)(tiles * splits), NTHR, 0, s>>>(
+            M, N, K, A, lda, B, ldb, C, ldc, tiles_m, run_if, part, kc, (int)tiles);
+        const long long total = (long long)M * N;
+        const int g = (int)std::min<long long>((total + 255) / 256, 1184);
+        split_reduce_kernel<TRI><<<g, 256, 0, s>>>(M, N, splits, part, C, ldc);
+    }
+}
+
+// K split for launches that fill less than a wave: chunks of whole K steps,
+// as many as give about two CTAs per SM (at most 8, at least 128 K each),
+// when the partial products fit in the scratch half; 1 = no split.
+int split_count(const hdbf_context* ctx, int M, int N, int K, bool tri, int* kc)
+{
+    if (!ctx->ws || ctx->run_if || K < 512) return 1;
+    const long long tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
+    long long tiles = tm * tn;
+    if (tri) {  // tiles on or below the diagonal
+        tiles = 0;
+        for (long long j = 0; j < tn; ++j) tiles += std::max<long long>(0, tm - j);
+    }
+    if (tiles >= ctx->sm_count) return 1;
+    int S = (int)std::min<long long>(8, (2LL * ctx->sm_count) / std::max<long long>(tiles, 1));
+    while (S > 1 && ((long long)S * M * N > (long long)kSplitFloats || K / S < 128)) --S;
+    if (S < 2) return 1;
+    *kc = ((K + S - 1) / S + BK - 1) / BK * BK;
+    return (K + *kc - 1) / *kc;
 }
 
 hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, int N, int K,
@@ -242,22 +354,27 @@ hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, in
     }
     ProfScope prof(ctx, kClsGemm, flops, 4.0 * ((double)M * K + (double)N * K + 2.0 * M * N), M,
                    N, K);
+    int kc = 0;
+    const int S = split_count(ctx, M, N, K, lower_only, &kc);
+    float* part = S > 1 ? ws_split(ctx) : nullptr;
+#define HDBF_SUB(MD, V, T) launch_sub<MD, V, T>(s, M, N, K, A, lda, B, ldb, C, ldc, ri, part, S, kc)
     if (mode == kNT) {
         if (vec) {
-            if (lower_only) launch_sub<kNT, true, true>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
-            else launch_sub<kNT, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+            if (lower_only) HDBF_SUB(kNT, true, true);
+            else HDBF_SUB(kNT, true, false);
         } else {
-            if (lower_only) launch_sub<kNT, false, true>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
-            else launch_sub<kNT, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+            if (lower_only) HDBF_SUB(kNT, false, true);
+            else HDBF_SUB(kNT, false, false);
         }
     } else if (mode == kNN) {
-        if (vec) launch_sub<kNN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
-        else launch_sub<kNN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+        if (vec) HDBF_SUB(kNN, true, false);
+        else HDBF_SUB(kNN, false, false);
     } else {
-        if (vec) launch_sub<kTN, true, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
-        else launch_sub<kTN, false, false>(s, M, N, K, A, lda, B, ldb, C, ldc, ri);
+        if (vec) HDBF_SUB(kTN, true, false);
+        else HDBF_SUB(kTN, false, false);
     }
-    ctx->launches++;
+#undef HDBF_SUB
+    ctx->launches += part ? 2 : 1;
     return last_cuda(ctx);
 }
 
