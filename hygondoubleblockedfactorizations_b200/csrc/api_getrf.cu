@@ -273,6 +273,7 @@ hdbf_status getrf_db_impl(hdbf_context* ctx, T* A, int lda, int n, int outer_nb,
                 const int group = (panels + kLaEvents - 2) / (kLaEvents - 1);
                 chunk_w = group * inner_nb;
                 NoSkinny ns(ctx);  // the panel chain may use the split-K scratch
+                SplitPlan sp(ctx, n - next, nsz, next);  // chunks sum as the whole GEMM
                 for (int c0 = 0; c0 < nsz; c0 += chunk_w) {
                     const int cw = std::min(chunk_w, nsz - c0);
                     HDBF_TRY(gemm_sub(ctx, true, false, n - next, cw, next, at(A, lda, next, 0),

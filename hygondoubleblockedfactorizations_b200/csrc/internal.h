@@ -91,6 +91,10 @@ struct hdbf_context {
     cudaEvent_t la_ev[hdbf::kLaEvents] = {};
     bool la_used = false;    // the graph being captured forked onto la_stream
     bool no_skinny = false;  // keep GEMMs off the shared split-K scratch
+    // K chunk of the FP32 GEMM split (SplitPlan): -1 decides per launch,
+    // 0 never splits, > 0 splits K into chunks of this many.  Column chunks of
+    // one GEMM take the whole GEMM's plan so their sums match it bit for bit.
+    int split_kc = -1;
     unsigned spin_limit = 0; // hdbf_set_wait_limit (0: default)
     // Conditional launches (RunIf): while set, the FP32 GEMM and the
     // diagonal-block kernel run only when *run_if != 0 (read on the device).
@@ -276,6 +280,22 @@ hdbf_status last_cuda(hdbf_context* ctx);
 hdbf_status sgemm_sub(hdbf_context* ctx, bool nn, bool lower_only, int M, int N, int K,
                       const float* A, long long lda, const float* B, long long ldb,
                       float* C, long long ldc);
+
+// K split of the FP32 GEMM of shape M x N x K (tri: lower-triangle mode):
+// the number of chunks (1 = no split) and, in *kc, their length.
+int split_count(const hdbf_context* ctx, int M, int N, int K, bool tri, int* kc);
+// While alive, every FP32 GEMM splits K as the GEMM of the given shape does.
+struct SplitPlan {
+    hdbf_context* ctx;
+    int saved;
+    SplitPlan(hdbf_context* c, int M, int N, int K) : ctx(c), saved(c->split_kc)
+    {
+        int kc = 0;
+        const int S = split_count(c, M, N, K, false, &kc);
+        c->split_kc = S > 1 ? kc : 0;
+    }
+    ~SplitPlan() { ctx->split_kc = saved; }
+};
 
 // Skinny update (N <= 32): mode 0 C -= A * B^T, 1 C -= A * B, 2 C -= A^T * B,
 // with the operand shapes of sgemm_sub / sgemm_sub_tn.  sgemm_launch routes

@@ -310,12 +310,21 @@ void launch_sub(cudaStream_t s, int M, int N, int K, const float* A, long long l
     }
 }
 
+}  // namespace
+
 // K split for launches that fill less than a wave: chunks of whole K steps,
 // as many as give about two CTAs per SM (at most 8, at least 128 K each),
 // when the partial products fit in the scratch half; 1 = no split.
 int split_count(const hdbf_context* ctx, int M, int N, int K, bool tri, int* kc)
 {
-    if (!ctx->ws || ctx->run_if || K < 512) return 1;
+    if (!ctx->ws || ctx->run_if) return 1;
+    if (ctx->split_kc >= 0) {  // the plan of a whole GEMM this launch is a part of
+        if (ctx->split_kc == 0) return 1;
+        *kc = ctx->split_kc;
+        const int S = (K + *kc - 1) / *kc;
+        return (S > 1 && (long long)S * M * N <= (long long)kSplitFloats) ? S : 1;
+    }
+    if (K < 512) return 1;
     const long long tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
     long long tiles = tm * tn;
     if (tri) {  // tiles on or below the diagonal
@@ -329,6 +338,8 @@ int split_count(const hdbf_context* ctx, int M, int N, int K, bool tri, int* kc)
     *kc = ((K + S - 1) / S + BK - 1) / BK * BK;
     return (K + *kc - 1) / *kc;
 }
+
+namespace {
 
 hdbf_status sgemm_launch(hdbf_context* ctx, int mode, bool lower_only, int M, int N, int K,
                          const float* A, long long lda, const float* B, long long ldb, float* C,
