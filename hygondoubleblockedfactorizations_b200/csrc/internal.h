@@ -95,6 +95,9 @@ struct hdbf_context {
     // 0 never splits, > 0 splits K into chunks of this many.  Column chunks of
     // one GEMM take the whole GEMM's plan so their sums match it bit for bit.
     int split_kc = -1;
+    // Tensor-core GEMM kernel: 0 persistent 128 x 256 tiles with two TMEM
+    // accumulators (default), 1 one 128 x 128 tile per CTA (HDBF_TC_KERNEL).
+    int tc_kernel = 0;
     unsigned spin_limit = 0; // hdbf_set_wait_limit (0: default)
     // Conditional launches (RunIf): while set, the FP32 GEMM and the
     // diagonal-block kernel run only when *run_if != 0 (read on the device).

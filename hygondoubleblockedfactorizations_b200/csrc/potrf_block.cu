@@ -73,24 +73,33 @@ __device__ void grid_barrier(Sync& s)
     __syncthreads();
 }
 
-// dst[k][m] = src(m, k) = src[k * ld + m] (column-major 64 x 64 tile, k-major
-// in shared memory); entries outside rows x cols are zero.
-__device__ __forceinline__ void load_kmajor(float* dst, const float* src, long long ld, int rows,
-                                            int cols)
+// Two 64 x 64 tiles into shared memory, every global load of the thread in
+// flight before the first shared store (the tiles live in L2, so the loads'
+// latency, not their bandwidth, sets the cost).  Tile X (X = A, B) is the
+// column-major block src (leading dimension ld, entries outside rows x cols
+// read as zero); TX = false stores it k-major, dst[k][m] = src(m, k), and
+// TX = true transposed, dst[k][n] = src(k, n), both with row pitch kLdS.
+struct TileSrc {
+    const float* src;
+    long long ld;
+    int rows, cols;
+};
+template <bool TA, bool TB>
+__device__ __forceinline__ void load_pair(float* dA, TileSrc a, float* dB, TileSrc b)
 {
-    for (int q = threadIdx.x; q < kT * kT; q += kThreads) {
-        const int k = q >> 6, m = q & 63;
-        dst[k * kLdS + m] = (m < rows && k < cols) ? __ldcg(src + (long long)k * ld + m) : 0.f;
+    constexpr int kPer = kT * kT / kThreads;  // 16 elements per thread and tile
+    float va[kPer], vb[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int q = threadIdx.x + u * kThreads, c = q >> 6, r = q & 63;
+        va[u] = (r < a.rows && c < a.cols) ? __ldcg(a.src + (long long)c * a.ld + r) : 0.f;
+        vb[u] = (r < b.rows && c < b.cols) ? __ldcg(b.src + (long long)c * b.ld + r) : 0.f;
     }
-}
-
-// dst[k][n] = src(k, n) = src[n * ld + k] (transposing load).
-__device__ __forceinline__ void load_trans(float* dst, const float* src, long long ld, int rows,
-                                           int cols)
-{
-    for (int q = threadIdx.x; q < kT * kT; q += kThreads) {
-        const int n = q >> 6, k = q & 63;
-        dst[k * kLdS + n] = (k < rows && n < cols) ? __ldcg(src + (long long)n * ld + k) : 0.f;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int q = threadIdx.x + u * kThreads, c = q >> 6, r = q & 63;
+        dA[TA ? r * kLdS + c : c * kLdS + r] = va[u];
+        dB[TB ? r * kLdS + c : c * kLdS + r] = vb[u];
     }
 }
 
@@ -112,9 +121,14 @@ __device__ __forceinline__ void tile_mma(float acc[4][4], const float* As, const
 }
 
 // Register-resident Cholesky of the nb x nb (nb <= 64) lower tile at T
-// (thread (r, g) holds T(r, g + 4i), i < 16).  Returns the first failing
-// column or -1 (uniform over the CTA).
-__device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_d)
+// (thread (r, g) holds T(r, g + 4i), i < 16) with one barrier per column:
+// column j is read from the column buffer of parity j & 1 (every thread
+// scales the entries it needs by the reciprocal pivot itself), and the
+// threads holding column j + 1 publish it, fully updated, into the other
+// parity during the same step.  The factor goes back to T and, zero-padded
+// to 64 x 64, into Ls (Ls[r * 65 + c]) for the inverse.  Returns the first
+// failing column or -1 (uniform over the CTA).
+__device__ int potf2_tile(float* T, long long ld, int nb, float (*colbuf)[kT], float* Ls)
 {
     const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
     float a[16];
@@ -123,58 +137,57 @@ __device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_
         const int c = g + 4 * i;
         a[i] = (r < nb && c < nb && r >= c) ? __ldcg(T + (long long)c * ld + r) : 0.f;
     }
+    if (g == 0) colbuf[0][r] = a[0];
+    __syncthreads();
     int failed_at = -1;
     for (int j = 0; j < nb; ++j) {
-        const int gj = j & 3, ij = j >> 2;
-        float own = 0.f;
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (i == ij) own = a[i];
-        if (g == gj && r == j) *s_d = own;
-        __syncthreads();
-        const float d = *s_d;
+        const float* cb = colbuf[j & 1];
+        const float d = cb[j];
         if (!(d > 0.f)) {
             failed_at = j;
             break;
         }
         const float sd = sqrtf(d);
         const float rcp = 1.0f / sd;
-        if (g == gj) {
-            const float v = (r == j) ? sd : (r > j ? own * rcp : own);
+        const int ij = j >> 2;
+        const float lr = cb[r] * rcp;  // L(r, j) for r > j
+        if (g == (j & 3)) {
 #pragma unroll
             for (int i = 0; i < 16; ++i)
-                if (i == ij) a[i] = v;
-            if (r > j) lcol[r] = v;
+                if (i == ij) a[i] = (r == j) ? sd : (r > j ? lr : a[i]);
         }
-        __syncthreads();
         if (r > j) {
-            const float lr = lcol[r];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int c = g + 4 * i;
-                if (c > j && c <= r) a[i] = fmaf(-lr, lcol[c], a[i]);
+                if (c > j && c <= r) a[i] = fmaf(-lr, cb[c] * rcp, a[i]);
             }
         }
+        const int jn = j + 1;
+        if (g == (jn & 3)) {
+            float own = 0.f;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (i == (jn >> 2)) own = a[i];
+            colbuf[jn & 1][r] = own;
+        }
+        __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         const int c = g + 4 * i;
         if (r < nb && c < nb && r >= c) T[(long long)c * ld + r] = a[i];
+        Ls[r * 65 + c] = a[i];  // zero outside the factor's lower triangle
     }
     return failed_at;
 }
 
-// D = L^{-1} for the nb x nb lower tile L (padded with the identity to 64):
-// thread t < 64 solves L x = e_t by forward substitution over a shared copy.
-// D is written column-major with leading dimension 64 (D[c * 64 + r]).
-__device__ void tri_inv_tile(const float* L, long long ld, int nb, float* Ls /*64 x 65*/,
-                             float* D)
+// D = L^{-1} for the nb x nb lower factor held zero-padded to 64 x 64 in Ls
+// (Ls[r * 65 + c], written before the last barrier): thread t < 64 solves
+// L x = e_t by forward substitution.  D is written column-major with leading
+// dimension 64 (D[c * 64 + r]).
+__device__ void tri_inv_tile(const float* Ls, int nb, float* D)
 {
-    for (int q = threadIdx.x; q < kT * kT; q += kThreads) {
-        const int c = q >> 6, r = q & 63;
-        Ls[r * 65 + c] = (r < nb && c < nb && r >= c) ? __ldcg(L + (long long)c * ld + r) : 0.f;
-    }
-    __syncthreads();
     const int t = threadIdx.x;
     if (t < kT) {
         float x[kT];
@@ -201,8 +214,7 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
 {
     __shared__ __align__(16) float As[kT * kLdS];
     __shared__ __align__(16) float Bs[kT * kLdS];
-    __shared__ float lcol[kT];
-    __shared__ float s_d;
+    __shared__ float colbuf[2][kT];
     __shared__ int s_flag;
     const int NT = (n + kT - 1) / kT;
     const int cta = blockIdx.x;
@@ -224,7 +236,7 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
 
     // Factor (and invert) diagonal tile k on this CTA; false on a bad pivot.
     auto factor_diag = [&](int k) -> bool {
-        const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d);
+        const int f = potf2_tile(tile(k, k), lda, ext(k), colbuf, As);
         if (f >= 0) {
             if (tid == 0) {
                 if (info) atomicCAS(info, 0, info_base + k * kT + f + 1);
@@ -233,26 +245,34 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
             return false;
         }
         __syncthreads();
-        tri_inv_tile(tile(k, k), lda, ext(k), As, dinv + (long long)k * kT * kT);
+        tri_inv_tile(As, ext(k), dinv + (long long)k * kT * kT);
         return true;
     };
     // A(i,j) -= L(i,k) L(j,k)^T (lower part only on the diagonal)
     auto update_tile = [&](int k, int i, int j) {
-        load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
-        load_kmajor(Bs, tile(j, k), lda, ext(j), ext(k));
+        load_pair<false, false>(As, {tile(i, k), lda, ext(i), ext(k)}, Bs,
+                                {tile(j, k), lda, ext(j), ext(k)});
         __syncthreads();
         float acc[4][4] = {};
         tile_mma(acc, As, Bs);
         float* T = tile(i, j);
+        float old[4][4];  // all loads in flight before the first store
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 const int r = ty * 4 + a, c = tx * 4 + b;
-                if (r < ext(i) && c < ext(j) && (i != j || r >= c)) {
-                    const long long o = (long long)c * lda + r;
-                    T[o] = __ldcg(T + o) - acc[a][b];
-                }
+                old[a][b] = (r < ext(i) && c < ext(j) && (i != j || r >= c))
+                                ? __ldcg(T + (long long)c * lda + r)
+                                : 0.f;
+            }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = ty * 4 + a, c = tx * 4 + b;
+                if (r < ext(i) && c < ext(j) && (i != j || r >= c))
+                    T[(long long)c * lda + r] = old[a][b] - acc[a][b];
             }
         __syncthreads();
     };
@@ -272,8 +292,8 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
     for (int k = 0; k < NT - 1 && ok; ++k) {
         // P2: L(i,k) = A(i,k) D_k^T for i > k
         for (int i = k + 1 + cta; i < NT; i += G) {
-            load_kmajor(As, tile(i, k), lda, ext(i), ext(k));
-            load_kmajor(Bs, dinv + (long long)k * kT * kT, kT, ext(k), ext(k));
+            load_pair<false, false>(As, {tile(i, k), lda, ext(i), ext(k)}, Bs,
+                                    {dinv + (long long)k * kT * kT, kT, ext(k), ext(k)});
             __syncthreads();
             float acc[4][4] = {};
             tile_mma(acc, As, Bs);
@@ -345,8 +365,8 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
             if (ci >= NT) continue;
             float acc[4][4] = {};
             for (int m = aj; m < b + st; ++m) {
-                load_kmajor(As, tile(ci, m), lda, ext(ci), ext(m));
-                load_trans(Bs, wt(m, aj), ldw, ext(m), ext(aj));
+                load_pair<false, true>(As, {tile(ci, m), lda, ext(ci), ext(m)}, Bs,
+                                       {wt(m, aj), ldw, ext(m), ext(aj)});
                 __syncthreads();
                 tile_mma(acc, As, Bs);
                 __syncthreads();
@@ -369,8 +389,8 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
             if (ci >= NT) continue;
             float acc[4][4] = {};
             for (int m = b + st; m <= ci; ++m) {
-                load_kmajor(As, wt(ci, m), ldw, ext(ci), ext(m));
-                load_trans(Bs, tt(m, aj), ldw, ext(m), ext(aj));
+                load_pair<false, true>(As, {wt(ci, m), ldw, ext(ci), ext(m)}, Bs,
+                                       {tt(m, aj), ldw, ext(m), ext(aj)});
                 __syncthreads();
                 tile_mma(acc, As, Bs);
                 __syncthreads();

@@ -395,6 +395,7 @@ hdbf_status hdbf_create(hdbf_handle* handle)
         if (v >= 64 && v <= 4096) ctx->panel_rows = v;
     }
     if (const char* la = std::getenv("HDBF_LOOKAHEAD")) ctx->lookahead = std::atoi(la) != 0;
+    if (const char* tk = std::getenv("HDBF_TC_KERNEL")) ctx->tc_kernel = std::atoi(tk) != 0;
     configure_tc_kernels(ctx);
     configure_trsm_block_kernels(ctx);
     configure_solve_kernels(ctx);
