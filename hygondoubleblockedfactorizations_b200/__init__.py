@@ -104,6 +104,7 @@ _PROTOS = {
                                     c_float, c_float, P, P]),
     "hdbf_selector_predict": (c_int, [P, P, P, P, c_int, c_int, c_int, P, P, P]),
     "hdbf_batched_num_variants": (c_int, []),
+    "hdbf_batched_variant_shape": (c_int, [c_int, P, P]),
     "hdbf_batched_factor_solve": (c_int, [P, c_int, c_int, P, P, P, P, P, P, P, P, P]),
     "launch_mixed_gemm": (None, [P, P, c_int, c_int, c_int, c_int, c_int, c_float, P, c_int, P,
                                  c_int, c_float, P, c_int]),

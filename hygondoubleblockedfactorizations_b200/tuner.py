@@ -1,8 +1,8 @@
 """Exhaustive autotuner.
 
-* ``tune_batched`` times every CTA-size variant of the persistent batched
-  kernel on a batch (inputs restored before each timed run) and returns the
-  fastest.
+* ``tune_batched`` times every launch shape of the persistent batched kernel
+  (threads per CTA x panel width, ``hdbf_batched_variant_shape``) on a batch
+  (inputs restored before each timed run) and returns the fastest.
 * ``tune_blocks`` times a grid of (outer block, inner block) choices for the
   large double-blocked factorizations at one order n and returns the fastest.
 * ``collect`` sweeps every candidate of the learned selector
@@ -191,11 +191,12 @@ def collect(torch, handle, nmax=32768, step=1024, mixes=48, heldout_mixes=16, se
         b = batch_mod.DeviceBatch(torch, ops, ns)
         batch_mod.fill_batch(torch, handle, b, seed + i)
         _, res = tune_batched(torch, handle, b, reps=1)
-        base = [k for k, c in enumerate(_candidates()) if c[0] == "variant"]
+        # the selector's batched candidates are the variants it names
+        cls = {c[1][0]: k for k, c in enumerate(_candidates()) if c[0] == "variant"}
         from .selector import order_stats
         recs.append({"op": "batched", "precision": "fp32", "stats": order_stats(ns),
                      "lu_fraction": float(ops.mean()), "heldout": held,
-                     "times": {str(base[v]): ms for v, ms in res.items()}})
+                     "times": {str(cls[v]): ms for v, ms in res.items() if v in cls}})
         if log:
             log("batched", len(ns), held, {v: round(ms, 3) for v, ms in res.items()})
         del b

@@ -13,10 +13,14 @@
  * failing column; queue is one DEVICE unsigned int the persistent CTAs use as
  * their work counter (reset by the call).
  *
- * variant selects the CTA size (0: 128, 1: 256, 2: 512 threads); the
- * autotuner (hygondoubleblockedfactorizations_b200.tuner) measures the
- * variants on a batch and picks one.  The launch (queue reset + kernel) is
- * recorded once per argument tuple as a CUDA graph and replayed afterwards.
+ * variant selects the launch shape: threads per CTA (one matrix per CTA at a
+ * time) and panel width, hdbf_batched_variant_shape; the panel width's
+ * shared-memory footprint sets how many CTAs share an SM.  Variants 0, 1, 2
+ * are 128, 256, 512 threads with 32-column panels; 3, 4, 5 the same with
+ * 16-column panels.  The autotuner (hygondoubleblockedfactorizations_b200.tuner)
+ * measures the variants on a batch and picks one.  The launch (queue reset +
+ * kernel) is recorded once per argument tuple as a CUDA graph and replayed
+ * afterwards.
  */
 #pragma once
 #include "hdbf/hdbf.h"
@@ -26,6 +30,9 @@ extern "C" {
 #endif
 
 int hdbf_batched_num_variants(void);
+
+/* Threads per CTA and panel width of a variant. */
+hdbf_status hdbf_batched_variant_shape(int variant, int* threads, int* panel);
 
 hdbf_status hdbf_batched_factor_solve(hdbf_handle handle, int variant, int count,
                                       const int* order, const int* op, const int* n,
