@@ -228,18 +228,15 @@ def cpu_baseline_and_check(n, A, G, gpu):
     del Lh
     rg_cpu = fp64_residual_device(LUh, G, pivh) / (n * 2.0 ** -23)
     del LUh
-    j, gap = oracle.pivot_divergence(G, pivh, gpu["ipiv"])
-    ok = (rp_gpu <= 10.0 and rg_gpu <= 10.0 and (j is None or gap < oracle.NEAR_TIE)
-          and gpu["info"] == [0, 0])
+    pv = oracle.pivot_agreement(G, pivh, gpu["ipiv"])
+    ok = rp_gpu <= 10.0 and rg_gpu <= 10.0 and pv["near_tie"] and gpu["info"] == [0, 0]
     check = {"ok": bool(ok), "n": n, "bound": 10.0, "eps": "2^-23",
              "what": "factors of the last timed step vs the CPU FP64 oracle and host LAPACK",
              "potrf_scaled_residual": round(rp_gpu, 5),
              "potrf_scaled_residual_host_lapack": round(rp_cpu, 5),
              "getrf_scaled_residual": round(rg_gpu, 5),
              "getrf_scaled_residual_host_lapack": round(rg_cpu, 5),
-             "pivots_vs_sgetrf": ("identical" if j is None else
-                                  {"first_divergence": j, "rel_gap": gap,
-                                   "near_tie": bool(gap < oracle.NEAR_TIE)}),
+             "pivots_vs_sgetrf": "identical" if pv["first_divergence"] is None else pv,
              "info": gpu["info"], "check_s": round(time.perf_counter() - t0, 1)}
     return base, check
 
@@ -722,10 +719,9 @@ def sweep(args):
         rg = oracle.scaled(oracle.getrf_residual_tiled(LU, G, ipiv), n)
         rgh = oracle.scaled(oracle.getrf_residual_tiled(LUh, G, pivh), n)
         del LU, LUh
-        j, gap = oracle.pivot_divergence(G, pivh, ipiv)
+        pv = oracle.pivot_agreement(G, pivh, ipiv)
         del G
-        ok = (info == [0, 0] and dev_err == 0 and rp <= 10.0 and rg <= 10.0
-              and (j is None or gap < oracle.NEAR_TIE))
+        ok = info == [0, 0] and dev_err == 0 and rp <= 10.0 and rg <= 10.0 and pv["near_tie"]
         pub = REF_PUBLISHED_SWEEP_MS.get(n, {})
         row.update({
             "ok": bool(ok),
@@ -735,9 +731,7 @@ def sweep(args):
             "getrf_tflops": round(flops_getrf(n) / (times["getrf"] / 1e3) / 1e12, 3),
             "potrf_scaled_residual": round(rp, 5), "potrf_scaled_residual_host_lapack": round(rph, 5),
             "getrf_scaled_residual": round(rg, 5), "getrf_scaled_residual_host_lapack": round(rgh, 5),
-            "pivots_vs_sgetrf": ("identical" if j is None else
-                                 {"first_divergence": j, "rel_gap": gap,
-                                  "near_tie": bool(gap < oracle.NEAR_TIE)}),
+            "pivots_vs_sgetrf": "identical" if pv["first_divergence"] is None else pv,
             "cpu_baseline": {"potrf_ms": round(1e3 * tp, 1), "getrf_ms": round(1e3 * tg, 1),
                              "potrf_tflops": round(flops_potrf(n) / tp / 1e12, 4),
                              "getrf_tflops": round(flops_getrf(n) / tg / 1e12, 4),

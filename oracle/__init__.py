@@ -16,7 +16,10 @@ Contents
   column by block column (host BLAS, a few FP64 blocks resident), for the
   orders 8192 ... 49152 of the sweep; pinned against the C version too.
 * ``pivot_divergence`` -- first index where two pivot sequences differ and the
-  FP64 relative gap of the two candidates there (near-tie test).
+  FP64 relative gap of the two candidates there.
+* ``pivot_agreement`` -- the same, plus the near-tie decision: the gap of the
+  two candidates against the rounding error an FP32 factorization commits in
+  them (unit roundoff x sqrt(j + 1) x (|a| + |L||U|) of the two rows).
 * ``double_blocked_potrf`` / ``double_blocked_getrf`` -- plain-C FP32 restatement
   of the reference loops (``factor.c``).
 * ``lapack_spotrf`` / ``lapack_sgetrf`` -- host LAPACK (SciPy's OpenBLAS), the
@@ -450,6 +453,87 @@ def pivot_divergence(A2d: np.ndarray, ipiv_a, ipiv_b):
 
 
 NEAR_TIE = 1e-4
+# A divergence is a near-tie when the two candidates' exact Schur-complement
+# magnitudes differ by less than TIE_ROUNDING times the typical rounding error
+# of a computed entry, u sqrt(j + 1) (|a_ij| + sum_k |l_ik| |u_kj|) (the
+# rounding-error bound of LU with the square-root growth of random rounding
+# errors in place of the worst-case j u).  Two FP32 implementations that sum
+# in different orders both commit that much, so either row is a correct
+# partial-pivoting choice within FP32 arithmetic.
+TIE_ROUNDING = 2.0
+
+
+def _lu_nopivot(M: np.ndarray) -> np.ndarray:
+    """In-place FP64 LU without pivoting of a square matrix whose rows are
+    already in pivot order (blocked right-looking, host BLAS)."""
+    from scipy.linalg import solve_triangular
+    n = M.shape[0]
+    nb = 128
+    for k in range(0, n, nb):
+        e = min(k + nb, n)
+        for c in range(k, e):
+            M[c + 1:, c] /= M[c, c]
+            M[c + 1:, c + 1:e] -= np.outer(M[c + 1:, c], M[c, c + 1:e])
+        if e < n:
+            M[k:e, e:] = solve_triangular(M[k:e, k:e], M[k:e, e:], lower=True,
+                                          unit_diagonal=True, check_finite=False)
+            M[e:, e:] -= M[e:, k:e] @ M[k:e, e:]
+    return M
+
+
+def pivot_agreement(A2d: np.ndarray, ipiv_ref, ipiv, unit_roundoff: float = 2.0 ** -24,
+                    rel_tie: float = NEAR_TIE) -> dict:
+    """Compare a pivot sequence with a reference one (both LAPACK 1-based).
+
+    Returns {"first_divergence": None} when identical; otherwise the first
+    differing column j, the FP64 relative gap of the two largest candidates
+    of the exact Schur complement column j (common pivot prefix applied),
+    "gap_over_rounding" = their absolute gap / (u sqrt(j + 1) s), s the larger
+    of |a_ij| + sum_k |l_ik| |u_kj| over the two rows (FP64 LU without
+    pivoting of the permuted leading block), and "near_tie": rel_gap < rel_tie
+    or gap_over_rounding <= TIE_ROUNDING.
+    """
+    from scipy.linalg import solve_triangular
+    a = np.asarray(ipiv_ref).astype(np.int64)
+    b = np.asarray(ipiv).astype(np.int64)
+    diff = np.nonzero(a != b)[0]
+    if diff.size == 0:
+        return {"first_divergence": None, "near_tie": True}
+    j = int(diff[0])
+    n = A2d.shape[0]
+    perm = np.arange(n)
+    for r in range(j):
+        p = a[r] - 1
+        perm[r], perm[p] = perm[p], perm[r]
+    M = np.asarray(A2d[:, : j + 1], dtype=np.float64)[perm, :]
+    if j > 0:
+        LU11 = _lu_nopivot(M[:j, :j].copy())
+        u12 = solve_triangular(LU11, M[:j, j], lower=True, unit_diagonal=True,
+                               check_finite=False)
+        x = solve_triangular(LU11, u12, lower=False, check_finite=False)
+        col = M[j:, j] - M[j:, :j] @ x  # Schur complement column j
+
+        def scale_of(i):  # |a_ij| + |l_i||u_j|, l_i = M[i, :j] U11^{-1}
+            li = solve_triangular(LU11, M[j + i, :j], trans="T", lower=False,
+                                  check_finite=False)
+            return float(abs(M[j + i, j]) + np.abs(li) @ np.abs(u12))
+    else:
+        col = M[:, 0].copy()
+
+        def scale_of(i):
+            return float(abs(col[i]))
+    order = np.argsort(-np.abs(col), kind="stable")
+    mag = np.abs(col)[order]
+    if mag.size < 2 or mag[0] == 0:
+        return {"first_divergence": j, "rel_gap": 0.0, "gap_over_rounding": 0.0,
+                "near_tie": True}
+    gap = float(mag[0] - mag[1])
+    rel = gap / float(mag[0])
+    s = max(scale_of(int(order[0])), scale_of(int(order[1])))
+    tau = unit_roundoff * np.sqrt(j + 1.0) * s
+    ratio = gap / tau if tau > 0 else float("inf")
+    return {"first_divergence": j, "rel_gap": rel, "gap_over_rounding": float(ratio),
+            "near_tie": bool(rel < rel_tie or ratio <= TIE_ROUNDING)}
 
 
 def parse_seed(text):

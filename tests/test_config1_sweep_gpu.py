@@ -77,8 +77,7 @@ def test_config1_getrf(hd, handle, torch_cuda, n):
     assert r <= BOUND, r
     _, piv_h, info_h = oracle.lapack_sgetrf(G)
     assert info_h == 0
-    j, gap = oracle.pivot_divergence(G, piv_h, piv)
-    if j is not None:
-        assert gap < oracle.NEAR_TIE, f"pivots diverge at {j} with gap {gap:.3g}"
+    pv = oracle.pivot_agreement(G, piv_h, piv)
+    assert pv["near_tie"], f"pivots diverge: {pv}"
     print(f"n={n}: GETRF scaled residual {r:.3g}; pivots vs sgetrf: "
-          + ("identical" if j is None else f"first divergence {j}, near-tie gap {gap:.2e}"))
+          + ("identical" if pv["first_divergence"] is None else f"near-tie divergence {pv}"))

@@ -52,9 +52,8 @@ def lu_resid(LU, A, ipiv):
 
 
 def assert_pivots64(A, ipiv, ref):
-    j, gap = oracle.pivot_divergence(A, ref, ipiv)
-    if j is not None:
-        assert gap < NEAR_TIE64, f"pivots diverge at {j} with gap {gap:.3g}"
+    pv = oracle.pivot_agreement(A, ref, ipiv, unit_roundoff=2.0 ** -53, rel_tie=NEAR_TIE64)
+    assert pv["near_tie"], f"pivots diverge: {pv}"
 
 
 POTRF_CASES = [

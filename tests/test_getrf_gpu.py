@@ -20,10 +20,11 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lapac
 
 def assert_pivots_match(G, ipiv, ref, what):
     """Identical pivots, or a first divergence at an FP32 near-tie (reported)."""
-    j, gap = oracle.pivot_divergence(G, ref, ipiv)
+    pv = oracle.pivot_agreement(G, ref, ipiv)
+    j = pv["first_divergence"]
     if j is not None:
-        assert gap < oracle.NEAR_TIE, f"{what}: pivots diverge at {j} with gap {gap:.3g}"
-        print(f"{what}: first divergence at column {j}, near-tie rel gap {gap:.2e}")
+        assert pv["near_tie"], f"{what}: pivots diverge: {pv}"
+        print(f"{what}: first divergence at column {j}, near-tie {pv}")
     return j
 
 

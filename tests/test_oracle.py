@@ -326,3 +326,28 @@ def test_recursive_potrf_matches_lapack(n, nb):
         A64[80, 80] = -1.0
         _, info = oracle.recursive_potrf(A64, nb, dtype=np.float64)
         assert info == lapack.dpotrf(np.asfortranarray(A64), lower=1)[1] == 81
+
+
+def test_pivot_agreement_rules():
+    """pivot_agreement: identical sequences; an exact tie (either row is a
+    correct partial-pivoting choice); a clear gap; and the rounding-scale rule
+    against the relative gap pivot_divergence reports."""
+    A = np.array([[1.0, 2.0, 0.5], [-1.0, 3.0, 1.0], [0.25, 1.0, 4.0]], dtype=np.float32)
+    assert oracle.pivot_agreement(A, [1, 2, 3], [1, 2, 3]) == {"first_divergence": None,
+                                                              "near_tie": True}
+    tie = oracle.pivot_agreement(A, [1, 2, 3], [2, 2, 3])  # |1| == |-1| in column 0
+    assert tie["first_divergence"] == 0 and tie["rel_gap"] == 0.0 and tie["near_tie"]
+    B = np.array([[1.0, 2.0], [4.0, 1.0]], dtype=np.float32)
+    far = oracle.pivot_agreement(B, [2, 2], [1, 2])
+    assert far["first_divergence"] == 0 and not far["near_tie"]
+    assert abs(far["rel_gap"] - 0.75) < 1e-12
+    # column 1 after a common first pivot: same gap as pivot_divergence
+    rng = np.random.default_rng(4)
+    C = rng.uniform(-1, 1, (6, 6)).astype(np.float32)
+    _, ref, _ = oracle.lapack_sgetrf(C)
+    other = ref.copy()
+    other[1] = 6 if ref[1] != 6 else 5
+    pa = oracle.pivot_agreement(C, ref, other)
+    j, gap = oracle.pivot_divergence(C, ref, other)
+    assert pa["first_divergence"] == j == 1 and abs(pa["rel_gap"] - gap) < 1e-12
+    assert pa["gap_over_rounding"] > 0
