@@ -386,6 +386,8 @@ def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
     def run(kind, A, B, X, prec, method):
         if method == "gmres":
             fn = "hdbf_dposv_mixed_gmres" if kind == "spd" else "hdbf_dgesv_mixed_gmres"
+        elif method == "auto":
+            fn = "hdbf_dposv_mixed_auto" if kind == "spd" else "hdbf_dgesv_mixed_auto"
         else:
             fn = "hdbf_dposv_mixed" if kind == "spd" else "hdbf_dgesv_mixed"
         info = hd.IrInfo()
@@ -393,6 +395,9 @@ def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
             args = (handle.ptr, hd.PREC[prec], A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
                     X.data_ptr(), n, ctypes.c_double(1e-13), 10, 30, ctypes.c_double(1e-4),
                     ctypes.byref(info))
+        elif method == "auto":
+            args = (handle.ptr, hd.PREC[prec], A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
+                    X.data_ptr(), n, ctypes.c_double(1e-13), 30, ctypes.byref(info))
         else:
             args = (handle.ptr, hd.PREC[prec], 1, A.data_ptr(), n, n, nrhs, B.data_ptr(), n,
                     X.data_ptr(), n, ctypes.c_double(1e-13), 30, ctypes.byref(info))
@@ -425,20 +430,9 @@ def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
             fp32_done[(kind, kappa)] = (min(ok, key=lambda c: c["ms"]) if ok else
                                         min(cand, key=lambda c: c["ms"]), cand)
         r32, alts = fp32_done[(kind, kappa)]
-        if method == "auto":
-            # classical refinement first; GMRES-IR when it does not converge
-            tried = [run(kind, A, B, X, prec, "ir")]
-            good = lambda c: (c["converged"] and c["backward_error"] <= 1e-13  # noqa: E731
-                              and c["backward_error_independent"] <= 1e-13)
-            if not good(tried[0]):
-                tried.append(run(kind, A, B, X, prec, "gmres"))
-            ok = [c for c in tried if good(c)]
-            rm = min(ok, key=lambda c: c["ms"]) if ok else tried[-1]
-            if len(tried) > 1:
-                rm = dict(rm, attempts=[{k: c[k] for k in ("method", "ms", "converged",
-                                                           "backward_error")} for c in tried])
-        else:
-            rm = run(kind, A, B, X, prec, method)
+        # "auto": the library's adaptive refinement (classical IR, then
+        # GMRES-IR, then a higher factorization precision), one call
+        rm = run(kind, A, B, X, prec, method)
         flops = (n ** 3 / 3.0) if kind == "spd" else (2.0 * n ** 3 / 3.0)
         key = f"{'potrf' if kind == 'spd' else 'getrf'}_k{kappa:.0e}_{prec}_{method}"
         out[key] = {
@@ -456,11 +450,13 @@ def config2(args):
     ``--config2``): n in {16384, 32768}, SPD and general A with singular
     values log-spaced in [1, kappa], kappa in {1e2, 1e4, 1e6}, BF16 and FP16
     trailing updates, nrhs = 16.  Each cell: the FP32 reference (faster
-    converged of classical IR and GMRES-IR), then the mixed factorization with
-    classical IR, falling back to GMRES-IR when classical refinement does not
-    reach 1e-13; refinement iterations, the library's and an independently
-    recomputed FP64 backward error, and the time-to-solution speed-up.  One
-    JSON line per order, then a summary."""
+    converged of classical IR and GMRES-IR), then one call of the library's
+    adaptive refinement from the mixed factorization (classical IR, GMRES-IR
+    from the first stalled step, a higher factorization precision when GMRES
+    stalls; hdbf_d{po,ge}sv_mixed_auto) to 1e-13; refinement iterations,
+    final precision, the library's and an independently recomputed FP64
+    backward error, and the time-to-solution speed-up.  One JSON line per
+    order, then a summary."""
     import torch
     import hygondoubleblockedfactorizations_b200 as hd
     torch.cuda.set_device(0)
@@ -474,6 +470,8 @@ def config2(args):
         for key, v in res.items():
             m = v["mixed_ir"]
             summary.append({"n": n, "cell": key, "method": m["method"],
+                            "final_precision": m["final_precision"],
+                            "factorizations": m["factorizations"],
                             "iterations": m["iterations"],
                             "inner_iterations": m["inner_iterations"],
                             "backward_error": m["backward_error"],

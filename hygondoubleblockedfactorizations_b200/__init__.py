@@ -98,6 +98,10 @@ _PROTOS = {
                                        c_double, c_int, c_int, c_double, P]),
     "hdbf_dgesv_mixed_gmres": (c_int, [P, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
                                        c_double, c_int, c_int, c_double, P]),
+    "hdbf_dposv_mixed_auto": (c_int, [P, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
+                                      c_double, c_int, P]),
+    "hdbf_dgesv_mixed_auto": (c_int, [P, c_int, P, c_int, c_int, c_int, P, c_int, P, c_int,
+                                      c_double, c_int, P]),
     "hdbf_selector_num_params": (c_int, [c_int, c_int]),
     "hdbf_selector_init": (c_int, [P, P, c_int, c_int, c_ull]),
     "hdbf_selector_train": (c_int, [P, P, P, P, c_int, P, P, P, c_int, c_int, c_int, c_int,

@@ -625,9 +625,16 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
 // GMRES-IR: x0 = M^{-1} b; per outer step r = b - A x (FP64), then restarted
 // left-preconditioned GMRES on M^{-1} A d = M^{-1} r (FP64 vectors, CGS2,
 // Givens least squares on the host per right-hand side), x += d.
+// Adaptive mode (`adaptive`): classical corrections d = M^{-1} r while each
+// one at least halves the backward error; from the first that does not,
+// GMRES steps on the same factors; when a GMRES step does not cut the
+// backward error tenfold, the factorization is redone at the next precision
+// (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3 -> FP32) and GMRES continues from
+// the current x.
 hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, int lda, int n,
                         int nrhs, const double* B, int ldb, double* X, int ldx, double tol,
-                        int max_iter, int max_inner, double inner_tol, hdbf_ir_info* out)
+                        int max_iter, int max_inner, double inner_tol, hdbf_ir_info* out,
+                        bool adaptive = false)
 {
     hdbf_ir_info info;
     memset(&info, 0, sizeof(info));
@@ -693,8 +700,21 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
         info.info = hinfo;
         info.fallback_panels = solver.fallbacks();
     }
+    int cur = prec;
+    if (adaptive) {
+        while (st == HDBF_STATUS_SUCCESS && hinfo != 0 && next_precision(cur) >= 0) {
+            // the panel fallback could not save it: refactor at the next precision
+            cur = next_precision(cur);
+            st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
+            info.factorizations++;
+            info.info = hinfo;
+            info.fallback_panels = solver.fallbacks();
+        }
+    }
     if (st == HDBF_STATUS_SUCCESS && hinfo == 0)
         st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });
+    bool classical = adaptive;
+    double prev = INFINITY;
     for (int it = 0; st == HDBF_STATUS_SUCCESS && hinfo == 0; ++it) {
         st = timed(&info.refine_ms, [&] { return solver.residual(); });
         if (st != HDBF_STATUS_SUCCESS) break;
@@ -715,6 +735,23 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             break;
         }
         if (it >= max_iter) break;
+        if (classical) {
+            if (berr < 0.5 * prev) {
+                prev = berr;
+                st = timed(&info.refine_ms,
+                           [&] { return solver.correction(buf.R, n, true); });
+                continue;
+            }
+            classical = false;  // stalled: GMRES on the same factors from here
+        } else if (adaptive && !(berr < 0.1 * prev) && next_precision(cur) >= 0) {
+            cur = next_precision(cur);
+            st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
+            info.factorizations++;
+            info.info = hinfo;
+            info.fallback_panels = solver.fallbacks();
+            if (st != HDBF_STATUS_SUCCESS || hinfo != 0) break;
+        }
+        prev = berr;
         // ---- inner GMRES on M^{-1} A d = M^{-1} r
         int steps = 0;
         st = timed(&info.refine_ms, [&]() -> hdbf_status {
@@ -787,7 +824,7 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
         });
         info.inner_iterations += steps;
     }
-    info.final_precision = prec;
+    info.final_precision = cur;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (out) *out = info;
@@ -870,6 +907,24 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle h, hdbf_precision prec, const dou
     if (!h) return HDBF_STATUS_INVALID_HANDLE;
     return h->last_status = gmres_mixed(h, false, prec, A, lda, n, nrhs, B, ldb, X, ldx, tol,
                                         max_iter, max_inner, inner_tol, out);
+}
+
+hdbf_status hdbf_dposv_mixed_auto(hdbf_handle h, hdbf_precision prec, const double* A, int lda,
+                                  int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                                  double tol, int max_iter, hdbf_ir_info* out)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = gmres_mixed(h, true, prec, A, lda, n, nrhs, B, ldb, X, ldx, tol,
+                                        max_iter, 30, 1e-4, out, true);
+}
+
+hdbf_status hdbf_dgesv_mixed_auto(hdbf_handle h, hdbf_precision prec, const double* A, int lda,
+                                  int n, int nrhs, const double* B, int ldb, double* X, int ldx,
+                                  double tol, int max_iter, hdbf_ir_info* out)
+{
+    if (!h) return HDBF_STATUS_INVALID_HANDLE;
+    return h->last_status = gmres_mixed(h, false, prec, A, lda, n, nrhs, B, ldb, X, ldx, tol,
+                                        max_iter, 30, 1e-4, out, true);
 }
 
 }  // extern "C"

@@ -93,6 +93,23 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, cons
                                    int ldx, double tol, int max_iter, int max_inner,
                                    double inner_tol, hdbf_ir_info* out);
 
+/* Adaptive refinement: one call that picks the refinement and, if needed, a
+ * higher factorization precision.  Classical corrections d = M^{-1} r while
+ * each at least halves the backward error; from the first that does not,
+ * GMRES-IR steps (30 inner steps, inner tolerance 1e-4) on the same factors;
+ * when a GMRES step does not cut the backward error tenfold, the matrix is
+ * refactored at the next precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3
+ * -> FP32; also when the factorization itself fails) and GMRES continues
+ * from the current solution.  Stops at tol or after max_iter outer steps;
+ * out->final_precision and out->factorizations record the escalations.
+ * nrhs <= 64. */
+hdbf_status hdbf_dposv_mixed_auto(hdbf_handle handle, hdbf_precision prec, const double* A,
+                                  int lda, int n, int nrhs, const double* B, int ldb, double* X,
+                                  int ldx, double tol, int max_iter, hdbf_ir_info* out);
+hdbf_status hdbf_dgesv_mixed_auto(hdbf_handle handle, hdbf_precision prec, const double* A,
+                                  int lda, int n, int nrhs, const double* B, int ldb, double* X,
+                                  int ldx, double tol, int max_iter, hdbf_ir_info* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -232,3 +232,46 @@ def test_wave_solve_repeated_launches(hd, handle, torch_cuda):
                                        B.astype(np.float64))
                 assert np.abs(X - want).max() <= 1e-4 * np.abs(want).max()
                 out[(n, nrhs)] = X
+
+
+def run_auto(hd, handle, torch, fn, A, B, prec, tol=1e-13, max_iter=30):
+    n, nrhs = B.shape
+    dA, dB = dev(torch, A), dev(torch, B)
+    dX = torch.zeros(n * nrhs, dtype=torch.float64, device="cuda")
+    info = hd_mod.IrInfo()
+    st = hd.call(fn, handle.ptr, hd_mod.PREC[prec], ptr(dA), n, n, nrhs, ptr(dB), n, ptr(dX), n,
+                 tol, max_iter, ctypes.byref(info))
+    torch.cuda.synchronize()
+    return st, host2d(dX, n, n, nrhs), info
+
+
+# Adaptive refinement: classical corrections while they halve the backward
+# error, then GMRES-IR, then a higher factorization precision.  A
+# well-conditioned SPD system finishes on classical steps alone; an
+# ill-conditioned general one (kappa = 1e6 is beyond BF16 factors, kappa *
+# u_bf16 ~ 4e3) needs GMRES and at least one refactorization, and still
+# reaches the FP64 target.
+def test_dposv_mixed_auto_classical_only(hd, handle, torch_cuda):
+    n, nrhs = 1024, 8
+    A = oracle.spd_kappa(n, 1e2, 11)
+    B = np.random.default_rng(12).standard_normal((n, nrhs))
+    st, X, info = run_auto(hd, handle, torch_cuda, "hdbf_dposv_mixed_auto", A, B, "fp16")
+    assert st == 0, hd_mod.status_string(st)
+    assert info.converged == 1 and info.inner_iterations == 0 and info.factorizations == 1
+    assert info.final_precision == hd_mod.PREC["fp16"]
+    assert oracle.backward_error(A, X, B) <= 1e-13
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp16"])
+def test_dgesv_mixed_auto_escalates(hd, handle, torch_cuda, prec):
+    n, nrhs = 1024, 8
+    A = oracle.general_kappa(n, 1e6, 21)
+    B = np.random.default_rng(22).standard_normal((n, nrhs))
+    st, X, info = run_auto(hd, handle, torch_cuda, "hdbf_dgesv_mixed_auto", A, B, prec)
+    assert st == 0, hd_mod.status_string(st)
+    assert info.converged == 1, (info.backward_error, list(info.history[:info.iterations + 1]),
+                                 info.final_precision, info.factorizations)
+    assert oracle.backward_error(A, X, B) <= 1e-13
+    chain = [prec, prec + "x3", "fp32"]  # the escalation order
+    assert info.final_precision == hd_mod.PREC[chain[info.factorizations - 1]], \
+        (info.final_precision, info.factorizations)
