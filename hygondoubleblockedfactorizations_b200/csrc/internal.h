@@ -255,7 +255,7 @@ struct WsLayout {
 // Split-K partial sums of under-filled FP32 GEMM launches: two halves of
 // kSplitFloats each, one for the handle's stream and one for its look-ahead
 // stream, so concurrent GEMMs on the two never share scratch.
-constexpr size_t kSplitFloats = (size_t)5 << 20;
+constexpr size_t kSplitFloats = (size_t)32 << 20;
 WsLayout ws_layout(int n);
 // Guarantee the layout for order n (grows the arena outside stream capture).
 hdbf_status ensure_ws(hdbf_context* ctx, int n);

@@ -312,9 +312,12 @@ void launch_sub(cudaStream_t s, int M, int N, int K, const float* A, long long l
 
 }  // namespace
 
-// K split for launches that fill less than a wave: chunks of whole K steps,
-// as many as give about two CTAs per SM (at most 8, at least 128 K each),
-// when the partial products fit in the scratch half; 1 = no split.
+// K split against wave quantisation: a launch whose last wave of CTAs would
+// leave SMs idle splits K into S chunks of whole K steps (at most 8, at least
+// 512 K each, 256 under one wave) when that shortens the wave-model time ceil(tiles S / slots)
+// x K / S (slots = two CTAs per SM) by at least 5% after a 3% charge per
+// extra chunk for the ordered reduction of the partial products, which must
+// fit in the scratch half; 1 = no split.
 int split_count(const hdbf_context* ctx, int M, int N, int K, bool tri, int* kc)
 {
     if (!ctx->ws || ctx->run_if) return 1;
@@ -331,11 +334,29 @@ int split_count(const hdbf_context* ctx, int M, int N, int K, bool tri, int* kc)
         tiles = 0;
         for (long long j = 0; j < tn; ++j) tiles += std::max<long long>(0, tm - j);
     }
-    if (tiles >= ctx->sm_count) return 1;
-    int S = (int)std::min<long long>(8, (2LL * ctx->sm_count) / std::max<long long>(tiles, 1));
-    while (S > 1 && ((long long)S * M * N > (long long)kSplitFloats || K / S < 128)) --S;
-    if (S < 2) return 1;
-    *kc = ((K + S - 1) / S + BK - 1) / BK * BK;
+    if (tiles <= 0) return 1;
+    const long long slots = 2LL * ctx->sm_count;
+    auto chunk = [&](int S) { return ((K + S - 1) / S + BK - 1) / BK * BK; };
+    auto cost = [&](int S) {
+        const int c = chunk(S);
+        const int parts = (K + c - 1) / c;
+        const long long waves = (tiles * parts + slots - 1) / slots;
+        return (double)waves * c * (1.0 + 0.03 * (parts - 1));
+    };
+    int best = 1;
+    double best_cost = cost(1);
+    for (int S = 2; S <= 8; ++S) {
+        // chunks of at least 512 K (256 when the launch fills under a wave)
+        if (K / S < (tiles < slots ? 256 : 512) || (long long)S * M * N > (long long)kSplitFloats)
+            break;
+        const double c = cost(S);
+        if (c < 0.95 * best_cost) {
+            best = S;
+            best_cost = c;
+        }
+    }
+    if (best < 2) return 1;
+    *kc = chunk(best);
     return (K + *kc - 1) / *kc;
 }
 
