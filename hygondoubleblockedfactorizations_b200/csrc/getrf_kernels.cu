@@ -129,7 +129,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                   int* info, int info_base, unsigned long long* scr, unsigned* epoch_ptr,
                   unsigned* done_ptr, int* err, int pivot)
 {
-    extern __shared__ float tile[];  // tile[c * rpc + r]
+    extern __shared__ float tile[];  // tile[c * ldt + r]
     __shared__ float prow_s[2][kCoopMaxW];  // finished pivot rows of the last two columns
     __shared__ float red_v[kCoopThreads / 32];
     __shared__ int red_i[kCoopThreads / 32];
@@ -145,6 +145,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int r0 = cta * rpc;
+    const int ldt = rpc | 1;
     const int nr = max(0, min(m, r0 + rpc) - r0);
     const int steps = min(m, w);
     const unsigned epoch = *reinterpret_cast<volatile unsigned*>(epoch_ptr);
@@ -171,7 +172,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         return v;
     };
 
-    coop_move<true>(A + r0, lda, tile, rpc, nr, w);
+    coop_move<true>(A + r0, lda, tile, ldt, nr, w);
     if (tid == 0) s_abort = 0;
     __syncthreads();
 
@@ -182,7 +183,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         int bi = INT_MAX;
         for (int r = tid; r < nr; r += kCoopThreads) {
             if (r0 + r >= col) {
-                const float v = fabsf(tile[col * rpc + r]);
+                const float v = fabsf(tile[col * ldt + r]);
                 if (bi == INT_MAX || v > bv) { bv = v; bi = r0 + r; }
             }
         }
@@ -209,10 +210,10 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         unsigned long long* slot = slot_of(col % kCoopSlots, cta);
         const unsigned long long t = (unsigned long long)row_tag(col) << 32;
         if (tid < w) {
-            if (lr >= 0) st_relaxed_u64(slot + 2 + tid, t | __float_as_uint(tile[tid * rpc + lr]));
+            if (lr >= 0) st_relaxed_u64(slot + 2 + tid, t | __float_as_uint(tile[tid * ldt + lr]));
             if (owns(col))
                 st_relaxed_u64(slot + 2 + kCoopMaxW + tid,
-                               t | __float_as_uint(tile[tid * rpc + (col - r0)]));
+                               t | __float_as_uint(tile[tid * ldt + (col - r0)]));
         }
         if (tid == 0) {
             const unsigned lo = ((unsigned)(col + 1) << 16) | (lr >= 0 ? (unsigned)lr : kNoRow);
@@ -262,7 +263,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                 if (polls > 256) __nanosleep(32);
             }
             cv[tid] = __uint_as_float((unsigned)(hv >> 32));
-            ci[tid] = none ? INT_MAX : tid * rpc + (int)((unsigned)hv & 0xffffu);
+            ci[tid] = none ? INT_MAX : tid * ldt + (int)((unsigned)hv & 0xffffu);
             cw[tid][0] = word_val(v0);
             cw[tid][1] = word_val(v1);
             cw[tid][2] = word_val(v2);
@@ -325,7 +326,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         auto place_diag_row = [&]() {
             if (tid < w && tid != j && tid != j + 1) {
                 wo = await_word(so + tid, wo, want);
-                tile[tid * rpc + (gi - r0)] = finish(word_val(wo), dw[0], tid);
+                tile[tid * ldt + (gi - r0)] = finish(word_val(wo), dw[0], tid);
             }
             diag_done = true;
         };
@@ -339,20 +340,20 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         for (int r = tid; r < nr; r += kCoopThreads) {
             const int g = r0 + r;
             if (own_j && g == j) {
-                tile[j * rpc + r] = piv;
-                if (has_next) tile[(j + 1) * rpc + r] = u1;
+                tile[j * ldt + r] = piv;
+                if (has_next) tile[(j + 1) * ldt + r] = u1;
             }
             if (own_g && g == gi) {
-                tile[j * rpc + r] = d0;
-                if (has_next) tile[(j + 1) * rpc + r] = d1;
+                tile[j * ldt + r] = d0;
+                if (has_next) tile[(j + 1) * ldt + r] = d1;
             }
             if (g > j) {
-                float l = tile[j * rpc + r];
+                float l = tile[j * ldt + r];
                 if (nz) {
                     l = recip ? l * rcp : l / piv;
-                    tile[j * rpc + r] = l;
+                    tile[j * ldt + r] = l;
                 }
-                if (has_next) tile[(j + 1) * rpc + r] = fmaf(-l, u1, tile[(j + 1) * rpc + r]);
+                if (has_next) tile[(j + 1) * ldt + r] = fmaf(-l, u1, tile[(j + 1) * ldt + r]);
             }
         }
         if (j + 1 < steps) {
@@ -376,30 +377,30 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
             wp = await_word(sw + tid, wp, want);
             const float pv = finish(word_val(wp), win[0], tid);
             prow[tid] = pv;
-            if (own_j) tile[tid * rpc + (j - r0)] = pv;
+            if (own_j) tile[tid * ldt + (j - r0)] = pv;
         }
         if (!diag_done) place_diag_row();
         __syncthreads();
         if (s_abort) break;
         for (int r = tid; r < nr; r += kCoopThreads) {
             if (r0 + r > j) {
-                const float l = tile[j * rpc + r];
+                const float l = tile[j * ldt + r];
                 int c = j + 2;
                 for (; c + 3 < w; c += 4) {
-                    const float t0 = tile[c * rpc + r], t1 = tile[(c + 1) * rpc + r];
-                    const float t2 = tile[(c + 2) * rpc + r], t3 = tile[(c + 3) * rpc + r];
-                    tile[c * rpc + r] = fmaf(-l, prow[c], t0);
-                    tile[(c + 1) * rpc + r] = fmaf(-l, prow[c + 1], t1);
-                    tile[(c + 2) * rpc + r] = fmaf(-l, prow[c + 2], t2);
-                    tile[(c + 3) * rpc + r] = fmaf(-l, prow[c + 3], t3);
+                    const float t0 = tile[c * ldt + r], t1 = tile[(c + 1) * ldt + r];
+                    const float t2 = tile[(c + 2) * ldt + r], t3 = tile[(c + 3) * ldt + r];
+                    tile[c * ldt + r] = fmaf(-l, prow[c], t0);
+                    tile[(c + 1) * ldt + r] = fmaf(-l, prow[c + 1], t1);
+                    tile[(c + 2) * ldt + r] = fmaf(-l, prow[c + 2], t2);
+                    tile[(c + 3) * ldt + r] = fmaf(-l, prow[c + 3], t3);
                 }
-                for (; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
+                for (; c < w; ++c) tile[c * ldt + r] = fmaf(-l, prow[c], tile[c * ldt + r]);
             }
         }
     }
     __syncthreads();
 
-    coop_move<false>(A + r0, lda, tile, rpc, nr, w);
+    coop_move<false>(A + r0, lda, tile, ldt, nr, w);
 
     // The last CTA to finish clears every header of this launch and moves
     // the epoch on.
@@ -838,7 +839,7 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     // instead of hanging if the grid cannot fit.
     const size_t smem_cap = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
     const size_t row_bytes = (size_t)w * sizeof(float);
-    const long long fit_rows = (long long)(smem_cap / row_bytes);
+    const long long fit_rows = (long long)(smem_cap / row_bytes) - 1;  // room for the odd pitch
     const int target = ctx->panel_rows > 0 ? ctx->panel_rows : 256;
     int G = (m + target - 1) / target;
     if (fit_rows > 0 && (m + fit_rows - 1) / fit_rows > G) G = (int)((m + fit_rows - 1) / fit_rows);
@@ -847,7 +848,7 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     if (G > kCoopThreads - 3) G = kCoopThreads - 3;  // one watcher thread per CTA + 3
     if (G < 1) G = 1;
     int rpc = (m + G - 1) / G;
-    size_t smem = (size_t)rpc * w * sizeof(float);
+    size_t smem = (size_t)(rpc | 1) * w * sizeof(float);  // odd leading dimension
     if (smem > smem_cap || rpc >= (int)kNoRow) return HDBF_STATUS_NOT_SUPPORTED;
     unsigned* epoch = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallEpoch);
     unsigned* done = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallDone);
