@@ -121,216 +121,91 @@ __device__ __forceinline__ void tile_mma(float acc[4][4], const float* As, const
 }
 
 // ------------------------------------------------- diagonal tile: L and L^-1
-// The nb x nb (nb <= 64) lower tile at T is factored and inverted by the
-// whole CTA in four 16-column blocks (shared memory S = tile, X = inverse,
-// both row-major with pitch kP; identity padding beyond nb):
-//   for each block: warp 0 factors the 16 x 16 diagonal block with
-//   shuffles (lane = row) and inverts it (lane = column); all threads solve
-//   the rows below against that inverse (L_r = A_r X_d^T) and apply the
-//   rank-16 update to the trailing lower triangle;
-// then L^-1 by recursive doubling, 16 -> 32 -> 64:
-//   X21 = -X22 (L21 X11).
-// Twelve barriers for the factorization, eight for the inverse, instead of a
-// barrier (or two) per column.
-constexpr int kP = 65;   // row pitch of S and X (odd: conflict-free rows and columns)
-constexpr int kDB = 16;  // diagonal block
+// Code size matters here: the tile routines run once per tile column, so a
+// long unrolled body is fetched from L2 every time.  Both keep compact loops.
 
-// Warp 0: Cholesky of the 16 x 16 diagonal block at (c0, c0) of S and its
-// inverse into X; returns the first failing column of the block or -1.
-__device__ int chol16_inv16(float* S, float* X, int c0)
+// Register-resident Cholesky of the nb x nb (nb <= 64) lower tile at T
+// (thread (r, g) holds T(r, g + 4i), i < 16).  The factor goes back to T
+// and, zero-padded to 64 x 64, into Ls (Ls[r * 65 + c]) for the inverse.
+// Returns the first failing column or -1 (uniform over the CTA).
+__device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_d, float* Ls)
 {
-    const int l = threadIdx.x & 31;
-    const int lr = l < kDB ? l : 0;  // lanes 16..31 mirror lane 0 (results unused)
-    float v[kDB];
+    const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
+    float a[16];
 #pragma unroll
-    for (int m = 0; m < kDB; ++m) v[m] = m <= lr ? S[(c0 + lr) * kP + c0 + m] : 0.f;
-    int fail = -1;
+    for (int i = 0; i < 16; ++i) {
+        const int c = g + 4 * i;
+        a[i] = (r < nb && c < nb && r >= c) ? __ldcg(T + (long long)c * ld + r) : 0.f;
+    }
+    int failed_at = -1;
+    for (int j = 0; j < nb; ++j) {
+        const int gj = j & 3, ij = j >> 2;
+        float own = 0.f;
 #pragma unroll
-    for (int j = 0; j < kDB; ++j) {
-        const float dj = __shfl_sync(0xffffffffu, v[j], j);
-        if (!(dj > 0.f)) {  // uniform in the warp
-            fail = j;
+        for (int i = 0; i < 16; ++i)
+            if (i == ij) own = a[i];
+        if (g == gj && r == j) *s_d = own;
+        __syncthreads();
+        const float d = *s_d;
+        if (!(d > 0.f)) {
+            failed_at = j;
             break;
         }
-        const float sd = sqrtf(dj);
+        const float sd = sqrtf(d);
         const float rcp = 1.0f / sd;
-        if (lr == j) v[j] = sd;
-        else if (lr > j) v[j] = v[j] * rcp;
+        if (g == gj) {
+            const float v = (r == j) ? sd : (r > j ? own * rcp : own);
 #pragma unroll
-        for (int c = j + 1; c < kDB; ++c) {
-            const float lc = __shfl_sync(0xffffffffu, v[j], c);
-            if (lr >= c) v[c] = fmaf(-v[j], lc, v[c]);
+            for (int i = 0; i < 16; ++i)
+                if (i == ij) a[i] = v;
+            if (r > j) lcol[r] = v;
+        }
+        __syncthreads();
+        if (r > j) {
+            const float lr = lcol[r];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int c = g + 4 * i;
+                if (c > j && c <= r) a[i] = fmaf(-lr, lcol[c], a[i]);
+            }
         }
     }
-    if (l < kDB) {
 #pragma unroll
-        for (int m = 0; m < kDB; ++m)
-            if (m <= l) S[(c0 + l) * kP + c0 + m] = v[m];
+    for (int i = 0; i < 16; ++i) {
+        const int c = g + 4 * i;
+        if (r < nb && c < nb && r >= c) T[(long long)c * ld + r] = a[i];
+        Ls[r * 65 + c] = a[i];  // zero outside the factor's lower triangle
     }
-    if (fail >= 0) return fail;
-    // inverse: lane t solves L x = e_t (column t of X_d), L(i, m) from lane i
-    const int t = lr;
-    float x[kDB];
-#pragma unroll
-    for (int i = 0; i < kDB; ++i) {
-        float acc = (i == t) ? 1.f : 0.f;
-#pragma unroll
-        for (int m = 0; m < i; ++m) acc = fmaf(-__shfl_sync(0xffffffffu, v[m], i), x[m], acc);
-        x[i] = acc / __shfl_sync(0xffffffffu, v[i], i);
-    }
-    if (l < kDB) {
-#pragma unroll
-        for (int i = 0; i < kDB; ++i) X[(c0 + i) * kP + c0 + l] = x[i];
-    }
-    return -1;
+    return failed_at;
 }
 
-// Factor the tile at T (nb <= 64) into S (lower, row-major pitch kP) and
-// invert it into X; L goes back to T and L^-1 (zero above the diagonal,
-// identity beyond nb) to D (column-major, leading dimension 64).  Returns the
-// first failing column or -1 (uniform over the CTA); on failure T holds the
-// partial factor and D is not written.
-__device__ int factor_invert_tile(float* T, long long ld, int nb, float* S, float* X, float* D,
-                                  int* s_fail)
+// D = L^{-1} for the nb x nb lower factor held zero-padded to 64 x 64 in Ls
+// (Ls[r * 65 + c]); the padding's diagonal counts as one.  Forward
+// substitution on the columns of D, four threads of one warp per column
+// (thread (t, q) keeps the rows i = q mod 4 of column t in Xs[i * 65 + t]);
+// per step k the owner of row k divides and the warp synchronises.  D is
+// written column-major with leading dimension 64 (D[c * 64 + r]).
+__device__ void tri_inv_tile(const float* Ls, int nb, float* Xs /*64 x 65*/, float* D)
 {
     const int tid = threadIdx.x;
-    {
-        float vv[kT * kT / kThreads];
-#pragma unroll
-        for (int u = 0; u < kT * kT / kThreads; ++u) {
-            const int q = tid + u * kThreads, c = q >> 6, r = q & 63;
-            vv[u] = (r < nb && c < nb && r >= c) ? __ldcg(T + (long long)c * ld + r)
-                                                 : (r == c ? 1.f : 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < kT * kT / kThreads; ++u) {
-            const int q = tid + u * kThreads, c = q >> 6, r = q & 63;
-            S[r * kP + c] = vv[u];
-            X[r * kP + c] = 0.f;
-        }
-    }
-    if (tid == 0) *s_fail = -1;
-    __syncthreads();
-    for (int kb = 0; kb < kT / kDB; ++kb) {
-        const int c0 = kb * kDB;
-        if (tid < 32) {
-            const int f = chol16_inv16(S, X, c0);
-            if (tid == 0 && f >= 0) *s_fail = c0 + f;
-        }
-        __syncthreads();
-        if (*s_fail >= 0) break;
-        const int rows = kT - c0 - kDB;  // rows below the block
-        if (rows > 0) {
-            // L_r = A_r X_d^T for rows r below: thread = (row, 4 columns)
-            const int r = c0 + kDB + (tid >> 2), g = tid & 3;
-            float out[4] = {0.f, 0.f, 0.f, 0.f};
-            if (tid < rows * 4) {
-                float a[kDB];
-#pragma unroll
-                for (int m = 0; m < kDB; ++m) a[m] = S[r * kP + c0 + m];
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) {
-                    const int j = g * 4 + jj;
-#pragma unroll
-                    for (int m = 0; m < kDB; ++m)
-                        if (m <= j) out[jj] = fmaf(a[m], X[(c0 + j) * kP + c0 + m], out[jj]);
-                }
-            }
-            __syncthreads();
-            if (tid < rows * 4) {
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) S[r * kP + c0 + g * 4 + jj] = out[jj];
-            }
-            __syncthreads();
-            // trailing lower triangle: S(r, c) -= sum_m L(r, c0+m) L(c, c0+m)
-            for (int idx = tid; idx < rows * rows; idx += kThreads) {
-                const int rr = idx / rows, cc = idx - rr * rows;
-                if (cc > rr) continue;
-                const int r2 = c0 + kDB + rr, c2 = c0 + kDB + cc;
-                float acc = S[r2 * kP + c2];
-#pragma unroll
-                for (int m = 0; m < kDB; ++m)
-                    acc = fmaf(-S[r2 * kP + c0 + m], S[c2 * kP + c0 + m], acc);
-                S[r2 * kP + c2] = acc;
-            }
-            __syncthreads();
-        }
-    }
-    const int fail = *s_fail;
-    // L back to T (lower part inside nb x nb)
-#pragma unroll
-    for (int u = 0; u < kT * kT / kThreads; ++u) {
-        const int q = tid + u * kThreads, c = q >> 6, r = q & 63;
-        if (r < nb && c < nb && r >= c) T[(long long)c * ld + r] = S[r * kP + c];
-    }
-    if (fail >= 0) return fail;
-    // L^-1 by recursive doubling: for sibling blocks of size h at b0 and
-    // b0 + h, X21 = -X22 (L21 X11); T21 = L21 X11 is kept in the X21 slot.
-    for (int h = kDB; h < kT; h *= 2) {
-        const int pairs = kT / (2 * h);
-        const int outs = pairs * h * h;  // outputs per phase
-        const int per = (outs + kThreads - 1) / kThreads;  // <= 4
-        float o[4];
-        // phase a: T21(i, j) = sum_{m >= j} L21(i, m) X11(m, j)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            o[u] = 0.f;
-            const int q = tid + u * kThreads;
-            if (u < per && q < outs) {
-                const int pr = q / (h * h), e = q - pr * h * h, i = e / h, j = e - i * h;
-                const int b0 = pr * 2 * h;
-                float acc = 0.f;
-                for (int m = j; m < h; ++m)
-                    acc = fmaf(S[(b0 + h + i) * kP + b0 + m], X[(b0 + m) * kP + b0 + j], acc);
-                o[u] = acc;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int q = tid + u * kThreads;
-            if (u < per && q < outs) {
-                const int pr = q / (h * h), e = q - pr * h * h, i = e / h, j = e - i * h;
-                const int b0 = pr * 2 * h;
-                X[(b0 + h + i) * kP + b0 + j] = o[u];
-            }
-        }
-        __syncthreads();
-        // phase b: X21(i, j) = -sum_{m <= i} X22(i, m) T21(m, j)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            o[u] = 0.f;
-            const int q = tid + u * kThreads;
-            if (u < per && q < outs) {
-                const int pr = q / (h * h), e = q - pr * h * h, i = e / h, j = e - i * h;
-                const int b0 = pr * 2 * h;
-                float acc = 0.f;
-                for (int m = 0; m <= i; ++m)
-                    acc = fmaf(X[(b0 + h + i) * kP + b0 + h + m], X[(b0 + h + m) * kP + b0 + j],
-                               acc);
-                o[u] = -acc;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int q = tid + u * kThreads;
-            if (u < per && q < outs) {
-                const int pr = q / (h * h), e = q - pr * h * h, i = e / h, j = e - i * h;
-                const int b0 = pr * 2 * h;
-                X[(b0 + h + i) * kP + b0 + j] = o[u];
-            }
-        }
-        __syncthreads();
-    }
-    // D (column-major, 64 x 64) = X
-#pragma unroll
-    for (int u = 0; u < kT * kT / kThreads; ++u) {
-        const int q = tid + u * kThreads, c = q >> 6, r = q & 63;
-        D[q] = X[r * kP + c];
+    const int t = tid >> 2, q = tid & 3;  // column, row class
+    for (int i = q; i < kT; i += 4) Xs[i * 65 + t] = (i == t) ? 1.f : 0.f;
+    __syncwarp();
+    for (int k = 0; k < kT; ++k) {
+        const float dk = k < nb ? Ls[k * 65 + k] : 1.f;
+        if ((k & 3) == q) Xs[k * 65 + t] = Xs[k * 65 + t] / dk;
+        __syncwarp();
+        const float xk = Xs[k * 65 + t];
+        const int first = k + 1 + ((q - (k + 1)) & 3);  // first row > k of class q
+        for (int i = first; i < kT; i += 4) Xs[i * 65 + t] = fmaf(-Ls[i * 65 + k], xk, Xs[i * 65 + t]);
+        __syncwarp();
     }
     __syncthreads();
-    return -1;
+    for (int e = tid; e < kT * kT; e += kThreads) {
+        const int c = e >> 6, r = e & 63;
+        D[e] = Xs[r * 65 + c];
+    }
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
@@ -340,7 +215,8 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
 {
     __shared__ __align__(16) float As[kT * kLdS];
     __shared__ __align__(16) float Bs[kT * kLdS];
-    __shared__ int s_tile_fail;
+    __shared__ float lcol[kT];
+    __shared__ float s_d;
     __shared__ int s_flag;
     const int NT = (n + kT - 1) / kT;
     const int cta = blockIdx.x;
@@ -362,8 +238,7 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
 
     // Factor (and invert) diagonal tile k on this CTA; false on a bad pivot.
     auto factor_diag = [&](int k) -> bool {
-        const int f = factor_invert_tile(tile(k, k), lda, ext(k), As, Bs,
-                                         dinv + (long long)k * kT * kT, &s_tile_fail);
+        const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d, As);
         if (f >= 0) {
             if (tid == 0) {
                 if (info) atomicCAS(info, 0, info_base + k * kT + f + 1);
@@ -371,6 +246,8 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
             }
             return false;
         }
+        __syncthreads();
+        tri_inv_tile(As, ext(k), Bs, dinv + (long long)k * kT * kT);
         return true;
     };
     // A(i,j) -= L(i,k) L(j,k)^T (lower part only on the diagonal)
