@@ -33,8 +33,6 @@ constexpr int kCoopMaxGrid = 256;
 // Per-(parity, CTA) exchange slot, in 64-bit words:
 // [header, pad | candidate row (kCoopMaxW) | diagonal row (kCoopMaxW)]
 constexpr int kSlotWords = 2 + 2 * kCoopMaxW;
-// Slot sets, used by columns j % kCoopSlots (see the protocol note).
-constexpr int kCoopSlots = 3;
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
 {
@@ -94,24 +92,15 @@ constexpr unsigned kNoRow = 0xffffu;  // "no candidate" in the header
 //   rows    [ tag : 32 | value bits : 32 ] for the CTA's candidate row and,
 //           from the CTA owning it, the diagonal row; tag = epoch << 8 |
 //           column + 1, epoch = launch counter.
-// Column j uses slot set j % 3.  Thread q of every CTA watches CTA q (bounded):
-// its header and, in the same L2 trip, its candidate row's entries in
-// columns j-1, j and j+1; three more threads read those entries of the
-// diagonal row.  That is all the critical path of a column needs: the pivot
-// (column j of the winner), the winner's column j+1 and the diagonal row's
-// columns j, j+1 (for the row that the swap moves), each finished with the
-// row's own column j-1 entry (see look-ahead below).  The full winner and
-// diagonal rows are loaded right after the reduction and consumed only by
-// the rest of the rank-1 update and the swap of the other columns, so their
-// latency overlaps the next column's work.  Each word proves its own
-// freshness (a reader re-reads any word whose tag is not yet this column's),
-// so a writer needs no release fence between its rows and its header.  A
-// CTA reads column j's words up to the end of its step j, i.e. before it
-// publishes column j + 2; a CTA rewrites set j % 3 only when it publishes
-// column j + 3, after it has seen every CTA's column-(j + 2) header, so three
-// sets suffice.  The last CTA to finish zeroes every header (column 0 never
-// matches) and advances the epoch, so no launch accepts an earlier launch's
-// words.
+// Column j uses parity j & 1.  Every CTA polls all G headers (thread q
+// watches CTA q, bounded) and then reads the winner's and the diagonal rows,
+// re-reading any word whose tag is not yet this column's: each word proves
+// its own freshness, so a writer needs no release fence between its rows and
+// its header, and one L2 trip delivers the flag with the candidate.  A CTA
+// only rewrites a parity after every CTA has published the following column,
+// i.e. after all of them finished reading it, so two parities suffice.  The
+// last CTA to finish zeroes every header (column 0 never matches) and
+// advances the epoch, so no launch accepts an earlier launch's words.
 //
 // Look-ahead inside the column loop: after the pivot of column j is applied,
 // each CTA updates only column j + 1 of its rows, publishes its column-(j+1)
@@ -119,33 +108,25 @@ constexpr unsigned kNoRow = 0xffffu;  // "no candidate" in the header
 // is in flight.  The published rows therefore still lack step j's update in
 // columns > j + 1; the receivers finish them with the row's own multiplier
 // (its column-j entry) and the step-j pivot row -- the same fmaf the owner
-// applies to its copy, so every CTA holds bit-identical rows.  A row that
-// the swap brings into a CTA is complete in columns j and j+1 at once; its
-// other columns are written when the full row has arrived, before the rest
-// of the update, or before the CTA publishes it if it becomes the next
-// candidate or diagonal row.
+// applies to its copy, so every CTA holds bit-identical rows.
 __global__ void __launch_bounds__(kCoopThreads)
 getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int ipiv_add,
                   int* info, int info_base, unsigned long long* scr, unsigned* epoch_ptr,
                   unsigned* done_ptr, int* err, int pivot)
 {
-    extern __shared__ float tile[];  // tile[c * ldt + r]
-    __shared__ float prow_s[2][kCoopMaxW];  // finished pivot rows of the last two columns
+    extern __shared__ float tile[];  // tile[c * rpc + r]
+    __shared__ float prow_s[2][kCoopMaxW];  // pivot rows of the last two columns
     __shared__ float red_v[kCoopThreads / 32];
     __shared__ int red_i[kCoopThreads / 32];
-    __shared__ float cv[kCoopMaxGrid];      // |candidate| of CTA q
-    __shared__ int ci[kCoopMaxGrid];        // its global row (INT_MAX: none)
-    __shared__ float cw[kCoopMaxGrid][3];   // its columns j-1, j, j+1 as published
-    __shared__ float dw[3];                 // the diagonal row's columns j-1, j, j+1
+    __shared__ float cv[kCoopMaxGrid];
+    __shared__ int ci[kCoopMaxGrid];
     __shared__ int s_abort, s_last;
 
     const int G = gridDim.x;
     const int cta = blockIdx.x;
     const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
+    const int lane = tid & 31, warp = tid >> 5;
     const int r0 = cta * rpc;
-    const int ldt = rpc | 1;
     const int nr = max(0, min(m, r0 + rpc) - r0);
     const int steps = min(m, w);
     const unsigned epoch = *reinterpret_cast<volatile unsigned*>(epoch_ptr);
@@ -154,25 +135,8 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         return scr + ((long long)par * kCoopMaxGrid + q) * kSlotWords;
     };
     auto row_tag = [&](int col) { return (epoch << 8) | (unsigned)(col + 1); };
-    auto owns = [&](int row) { return row >= r0 && row < r0 + nr; };
-    auto word_val = [](unsigned long long v) { return __uint_as_float((unsigned)v); };
-    auto word_tag = [](unsigned long long v) { return (unsigned)(v >> 32); };
-    // Bounded re-read of a row word until it carries tag `want`.
-    auto await_word = [&](const unsigned long long* p, unsigned long long v,
-                          unsigned want) -> unsigned long long {
-        unsigned polls = 0;
-        while (word_tag(v) != want) {
-            if (++polls > spin) {
-                atomicCAS(err, 0, kErrTimeout);
-                s_abort = 1;
-                break;
-            }
-            v = ld_relaxed_u64(p);
-        }
-        return v;
-    };
 
-    coop_move<true>(A + r0, lda, tile, ldt, nr, w);
+    coop_move<true>(A + r0, lda, tile, rpc, nr, w);
     if (tid == 0) s_abort = 0;
     __syncthreads();
 
@@ -183,7 +147,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         int bi = INT_MAX;
         for (int r = tid; r < nr; r += kCoopThreads) {
             if (r0 + r >= col) {
-                const float v = fabsf(tile[col * ldt + r]);
+                const float v = fabsf(tile[col * rpc + r]);
                 if (bi == INT_MAX || v > bv) { bv = v; bi = r0 + r; }
             }
         }
@@ -207,13 +171,14 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     // Publish column `col`: candidate row (local index lr, or -1), the
     // diagonal row if owned, and the header (no ordering needed among them).
     auto publish = [&](int col, int lr, float val) {
-        unsigned long long* slot = slot_of(col % kCoopSlots, cta);
+        unsigned long long* slot = slot_of(col & 1, cta);
         const unsigned long long t = (unsigned long long)row_tag(col) << 32;
+        const bool own_diag = col >= r0 && col < r0 + nr;
         if (tid < w) {
-            if (lr >= 0) st_relaxed_u64(slot + 2 + tid, t | __float_as_uint(tile[tid * ldt + lr]));
-            if (owns(col))
+            if (lr >= 0) st_relaxed_u64(slot + 2 + tid, t | __float_as_uint(tile[tid * rpc + lr]));
+            if (own_diag)
                 st_relaxed_u64(slot + 2 + kCoopMaxW + tid,
-                               t | __float_as_uint(tile[tid * ldt + (col - r0)]));
+                               t | __float_as_uint(tile[tid * rpc + (col - r0)]));
         }
         if (tid == 0) {
             const unsigned lo = ((unsigned)(col + 1) << 16) | (lr >= 0 ? (unsigned)lr : kNoRow);
@@ -231,30 +196,15 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     }
 
     for (int j = 0; j < steps; ++j) {
-        const int par = j % kCoopSlots;
+        const int par = j & 1;
         const unsigned tag = (unsigned)j + 1u;
-        const unsigned want = row_tag(j);
-        const int owner = j / rpc;
-        const bool has_next = j + 1 < w;
 
-        // 1. thread q < G: CTA q's header and its candidate's columns j-1,
-        // j, j+1; the last three threads: the diagonal row's (bounded)
-        if (tid < G) {
-            const unsigned long long* sq = slot_of(par, tid);
-            const unsigned long long* rq = sq + 2;
+        // 1. every candidate header of column j (thread q watches CTA q), bounded
+        for (int q = tid; q < G; q += kCoopThreads) {
+            const unsigned long long* wq = slot_of(par, q);
             unsigned polls = 0;
-            unsigned long long hv, v0 = 0ull, v1, v2 = 0ull;
-            bool none;
-            for (;;) {
-                hv = ld_relaxed_u64(sq);
-                if (j > 0) v0 = ld_relaxed_u64(rq + (j - 1));
-                v1 = ld_relaxed_u64(rq + j);
-                if (has_next) v2 = ld_relaxed_u64(rq + (j + 1));
-                none = ((unsigned)hv & 0xffffu) == kNoRow;
-                const bool hok = ((unsigned)(hv >> 16) & 0xffffu) == tag;
-                const bool rok = (j == 0 || word_tag(v0) == want) && word_tag(v1) == want &&
-                                 (!has_next || word_tag(v2) == want);
-                if (hok && (none || rok)) break;
+            unsigned long long wv;
+            while (((unsigned)((wv = ld_relaxed_u64(wq)) >> 16) & 0xffffu) != tag) {
                 if (++polls > spin) {
                     atomicCAS(err, 0, kErrTimeout);
                     s_abort = 1;
@@ -262,98 +212,91 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
                 }
                 if (polls > 256) __nanosleep(32);
             }
-            cv[tid] = __uint_as_float((unsigned)(hv >> 32));
-            ci[tid] = none ? INT_MAX : tid * ldt + (int)((unsigned)hv & 0xffffu);
-            cw[tid][0] = word_val(v0);
-            cw[tid][1] = word_val(v1);
-            cw[tid][2] = word_val(v2);
-        } else if (tid >= kCoopThreads - 3) {
-            const int e = tid - (kCoopThreads - 3), c = j - 1 + e;
-            float v = 0.f;
-            if (c >= 0 && c < w) {
-                const unsigned long long* p = slot_of(par, owner) + 2 + kCoopMaxW + c;
-                v = word_val(await_word(p, ld_relaxed_u64(p), want));
-            }
-            dw[e] = v;
+            const unsigned lr = (unsigned)wv & 0xffffu;
+            cv[q] = __uint_as_float((unsigned)(wv >> 32));
+            ci[q] = lr == kNoRow ? INT_MAX : q * rpc + (int)lr;
         }
         __syncthreads();
         if (s_abort) break;
 
-        // 2. the winner (every warp reduces the same candidates), the pivot,
-        // the winner's column j+1 and the diagonal row's columns j, j+1,
-        // finished with step j-1 (prev: its pivot row)
-        const float* prev = prow_s[(j & 1) ^ 1];
-        float* prow = prow_s[j & 1];
-        int gi = j, gc = owner;
-        if (pivot) {
-            float gv = -1.f;
-            gi = INT_MAX;
-            for (int q = lane; q < G; q += 32)
-                if (better(cv[q], ci[q], gv, gi)) { gv = cv[q]; gi = ci[q]; gc = q; }
+        // 2. the winner (each of the first warps reduces redundantly), its
+        // row and the diagonal row, finished with step j-1's update; swap.
+        const int owner = j / rpc;
+        float* prow = prow_s[par];
+        const float* prev = prow_s[par ^ 1];
+        if (tid < ((w + 31) & ~31)) {
+            int gi = j, gc = owner;
+            if (pivot) {
+                float gv = -1.f;
+                gi = INT_MAX;
+                for (int q = lane; q < G; q += 32)
+                    if (better(cv[q], ci[q], gv, gi)) { gv = cv[q]; gi = ci[q]; gc = q; }
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const float ov = __shfl_xor_sync(0xffffffffu, gv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, gi, off);
-                const int oc = __shfl_xor_sync(0xffffffffu, gc, off);
-                if (better(ov, oi, gv, gi)) { gv = ov; gi = oi; gc = oc; }
+                for (int off = 16; off > 0; off >>= 1) {
+                    const float ov = __shfl_xor_sync(0xffffffffu, gv, off);
+                    const int oi = __shfl_xor_sync(0xffffffffu, gi, off);
+                    const int oc = __shfl_xor_sync(0xffffffffu, gc, off);
+                    if (better(ov, oi, gv, gi)) { gv = ov; gi = oi; gc = oc; }
+                }
+                if (gi == INT_MAX) { gi = j; gc = owner; }  // unreachable: row j always competes
             }
-            if (gi == INT_MAX) { gi = j; gc = owner; }  // unreachable: row j always competes
-        }
-        const float* win = pivot && gi != j ? cw[gc] : dw;  // the pivot row's columns
-        auto finish = [&](float pub, float mult, int c) {
-            return (j > 0 && c > j) ? fmaf(-mult, prev[c], pub) : pub;
-        };
-        const float piv = win[1];
-        const float u1 = has_next ? finish(win[2], win[0], j + 1) : 0.f;
-        const float d0 = dw[1];
-        const float d1 = has_next ? finish(dw[2], dw[0], j + 1) : 0.f;
-        if (tid == 0 && pivot && cta == 0) ipiv[j] = gi + 1 + ipiv_add;
-        const bool swap = gi != j;
-        const bool own_j = swap && owns(j), own_g = swap && owns(gi);
-
-        // full pivot and diagonal rows: in flight until step 4
-        const unsigned long long* sw =
-            pivot && swap ? slot_of(par, gc) + 2 : slot_of(par, owner) + 2 + kCoopMaxW;
-        const unsigned long long* so = slot_of(par, owner) + 2 + kCoopMaxW;
-        unsigned long long wp = 0ull, wo = 0ull;
-        if (tid < w) {
-            wp = ld_relaxed_u64(sw + tid);
-            if (own_g) wo = ld_relaxed_u64(so + tid);
-        }
-        // The diagonal row moved into row gi: columns other than j, j+1
-        // (those are written in step 3), once its words have arrived.
-        bool diag_done = !own_g;
-        auto place_diag_row = [&]() {
-            if (tid < w && tid != j && tid != j + 1) {
-                wo = await_word(so + tid, wo, want);
-                tile[tid * ldt + (gi - r0)] = finish(word_val(wo), dw[0], tid);
+            if (tid < w) {
+                // without pivoting the pivot row is the diagonal row
+                const unsigned long long* sw =
+                    pivot ? slot_of(par, gc) + 2 : slot_of(par, owner) + 2 + kCoopMaxW;
+                const unsigned long long* so = slot_of(par, owner) + 2 + kCoopMaxW;
+                const unsigned want = row_tag(j);
+                const bool fin = j > 0 && tid > j;
+                unsigned long long wp = ld_relaxed_u64(sw + tid), wo = ld_relaxed_u64(so + tid);
+                unsigned long long wl = fin ? ld_relaxed_u64(sw + (j - 1)) : 0ull;
+                unsigned long long wm = fin ? ld_relaxed_u64(so + (j - 1)) : 0ull;
+                unsigned polls = 0;
+                while ((unsigned)(wp >> 32) != want || (unsigned)(wo >> 32) != want ||
+                       (fin && ((unsigned)(wl >> 32) != want || (unsigned)(wm >> 32) != want))) {
+                    if (++polls > spin) {
+                        atomicCAS(err, 0, kErrTimeout);
+                        s_abort = 1;
+                        break;
+                    }
+                    wp = ld_relaxed_u64(sw + tid);
+                    wo = ld_relaxed_u64(so + tid);
+                    if (fin) {
+                        wl = ld_relaxed_u64(sw + (j - 1));
+                        wm = ld_relaxed_u64(so + (j - 1));
+                    }
+                }
+                float pv = __uint_as_float((unsigned)wp), ov = __uint_as_float((unsigned)wo);
+                if (fin) {
+                    pv = fmaf(-__uint_as_float((unsigned)wl), prev[tid], pv);
+                    ov = fmaf(-__uint_as_float((unsigned)wm), prev[tid], ov);
+                }
+                prow[tid] = pv;
+                if (gi != j) {
+                    if (j >= r0 && j < r0 + nr) tile[tid * rpc + (j - r0)] = pv;
+                    if (gi >= r0 && gi < r0 + nr) tile[tid * rpc + (gi - r0)] = ov;
+                }
             }
-            diag_done = true;
-        };
+            if (tid == 0 && pivot && cta == 0) ipiv[j] = gi + 1 + ipiv_add;
+        }
+        __syncthreads();
+        if (s_abort) break;
 
-        // 3. swap columns j, j+1; scale column j, update column j+1 and find
-        // its candidate
+        // 3. scale column j, update column j+1 and find its candidate
+        const float piv = prow[j];
         const bool nz = piv != 0.f;
         const bool recip = fabsf(piv) >= FLT_MIN;
         const float rcp = 1.0f / piv;
         if (!nz && cta == 0 && tid == 0 && info) atomicCAS(info, 0, info_base + j + 1);
+        const bool next = j + 1 < w;
+        const float pn = next ? prow[j + 1] : 0.f;
         for (int r = tid; r < nr; r += kCoopThreads) {
-            const int g = r0 + r;
-            if (own_j && g == j) {
-                tile[j * ldt + r] = piv;
-                if (has_next) tile[(j + 1) * ldt + r] = u1;
-            }
-            if (own_g && g == gi) {
-                tile[j * ldt + r] = d0;
-                if (has_next) tile[(j + 1) * ldt + r] = d1;
-            }
-            if (g > j) {
-                float l = tile[j * ldt + r];
+            if (r0 + r > j) {
+                float l = tile[j * rpc + r];
                 if (nz) {
                     l = recip ? l * rcp : l / piv;
-                    tile[j * ldt + r] = l;
+                    tile[j * rpc + r] = l;
                 }
-                if (has_next) tile[(j + 1) * ldt + r] = fmaf(-l, u1, tile[(j + 1) * ldt + r]);
+                if (next) tile[(j + 1) * rpc + r] = fmaf(-l, pn, tile[(j + 1) * rpc + r]);
             }
         }
         if (j + 1 < steps) {
@@ -361,46 +304,29 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
             int lr = -1;
             if (pivot) lr = block_candidate(j + 1, v);  // its barrier orders the updates above
             else __syncthreads();
-            // the moved-in diagonal row is about to be published: complete it first
-            if (own_g && ((lr >= 0 && r0 + lr == gi) || gi == j + 1)) {
-                place_diag_row();
-                __syncthreads();
-            }
             publish(j + 1, lr, v);
         }
-        if (s_abort) break;
 
-        // 4. the full pivot row (finished) and the swapped rows' other
-        // columns, then the rest of step j's rank-1 update, overlapping the
-        // exchange of column j+1
-        if (tid < w) {
-            wp = await_word(sw + tid, wp, want);
-            const float pv = finish(word_val(wp), win[0], tid);
-            prow[tid] = pv;
-            if (own_j) tile[tid * ldt + (j - r0)] = pv;
-        }
-        if (!diag_done) place_diag_row();
-        __syncthreads();
-        if (s_abort) break;
+        // 4. the rest of step j's rank-1 update, overlapping the exchange
         for (int r = tid; r < nr; r += kCoopThreads) {
             if (r0 + r > j) {
-                const float l = tile[j * ldt + r];
+                const float l = tile[j * rpc + r];
                 int c = j + 2;
                 for (; c + 3 < w; c += 4) {
-                    const float t0 = tile[c * ldt + r], t1 = tile[(c + 1) * ldt + r];
-                    const float t2 = tile[(c + 2) * ldt + r], t3 = tile[(c + 3) * ldt + r];
-                    tile[c * ldt + r] = fmaf(-l, prow[c], t0);
-                    tile[(c + 1) * ldt + r] = fmaf(-l, prow[c + 1], t1);
-                    tile[(c + 2) * ldt + r] = fmaf(-l, prow[c + 2], t2);
-                    tile[(c + 3) * ldt + r] = fmaf(-l, prow[c + 3], t3);
+                    const float t0 = tile[c * rpc + r], t1 = tile[(c + 1) * rpc + r];
+                    const float t2 = tile[(c + 2) * rpc + r], t3 = tile[(c + 3) * rpc + r];
+                    tile[c * rpc + r] = fmaf(-l, prow[c], t0);
+                    tile[(c + 1) * rpc + r] = fmaf(-l, prow[c + 1], t1);
+                    tile[(c + 2) * rpc + r] = fmaf(-l, prow[c + 2], t2);
+                    tile[(c + 3) * rpc + r] = fmaf(-l, prow[c + 3], t3);
                 }
-                for (; c < w; ++c) tile[c * ldt + r] = fmaf(-l, prow[c], tile[c * ldt + r]);
+                for (; c < w; ++c) tile[c * rpc + r] = fmaf(-l, prow[c], tile[c * rpc + r]);
             }
         }
     }
     __syncthreads();
 
-    coop_move<false>(A + r0, lda, tile, ldt, nr, w);
+    coop_move<false>(A + r0, lda, tile, rpc, nr, w);
 
     // The last CTA to finish clears every header of this launch and moves
     // the epoch on.
@@ -411,7 +337,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
     }
     __syncthreads();
     if (s_last) {
-        for (int q = tid; q < kCoopSlots * G; q += kCoopThreads) *slot_of(q / G, q % G) = 0ull;
+        for (int q = tid; q < 2 * G; q += kCoopThreads) *slot_of(q / G, q % G) = 0ull;
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -420,6 +346,7 @@ getf2_coop_kernel(int m, int w, float* A, long long lda, int rpc, int* ipiv, int
         }
     }
 }
+
 // ------------------------------------------------------------ compose swaps
 constexpr int kComposeThreads = 1024;
 constexpr int kComposeMaxK = 4096;  // swaps composed by the sorted-group kernels
@@ -820,8 +747,7 @@ void configure_getrf_kernels(hdbf_context* ctx)
 
 size_t getf2_coop_scratch_bytes()
 {
-    return align_up((size_t)(kCoopSlots * kCoopMaxGrid * kSlotWords) * sizeof(unsigned long long),
-                    256);
+    return align_up((size_t)(2 * kCoopMaxGrid * kSlotWords) * sizeof(unsigned long long), 256);
 }
 
 hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda, int* ipiv,
@@ -839,16 +765,15 @@ hdbf_status getf2_coop(hdbf_context* ctx, int m, int w, float* A, long long lda,
     // instead of hanging if the grid cannot fit.
     const size_t smem_cap = ctx->max_smem_optin > 8192 ? ctx->max_smem_optin - 8192 : 40960;
     const size_t row_bytes = (size_t)w * sizeof(float);
-    const long long fit_rows = (long long)(smem_cap / row_bytes) - 1;  // room for the odd pitch
+    const long long fit_rows = (long long)(smem_cap / row_bytes);
     const int target = ctx->panel_rows > 0 ? ctx->panel_rows : 256;
     int G = (m + target - 1) / target;
     if (fit_rows > 0 && (m + fit_rows - 1) / fit_rows > G) G = (int)((m + fit_rows - 1) / fit_rows);
     if (G > ctx->sm_count) G = ctx->sm_count;
     if (G > kCoopMaxGrid) G = kCoopMaxGrid;
-    if (G > kCoopThreads - 3) G = kCoopThreads - 3;  // one watcher thread per CTA + 3
     if (G < 1) G = 1;
     int rpc = (m + G - 1) / G;
-    size_t smem = (size_t)(rpc | 1) * w * sizeof(float);  // odd leading dimension
+    size_t smem = (size_t)rpc * w * sizeof(float);
     if (smem > smem_cap || rpc >= (int)kNoRow) return HDBF_STATUS_NOT_SUPPORTED;
     unsigned* epoch = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallEpoch);
     unsigned* done = reinterpret_cast<unsigned*>(ctx->dev_small + kSmallDone);
