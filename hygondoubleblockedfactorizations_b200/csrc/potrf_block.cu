@@ -120,15 +120,10 @@ __device__ __forceinline__ void tile_mma(float acc[4][4], const float* As, const
     }
 }
 
-// ------------------------------------------------- diagonal tile: L and L^-1
-// Code size matters here: the tile routines run once per tile column, so a
-// long unrolled body is fetched from L2 every time.  Both keep compact loops.
-
 // Register-resident Cholesky of the nb x nb (nb <= 64) lower tile at T
-// (thread (r, g) holds T(r, g + 4i), i < 16).  The factor goes back to T
-// and, zero-padded to 64 x 64, into Ls (Ls[r * 65 + c]) for the inverse.
-// Returns the first failing column or -1 (uniform over the CTA).
-__device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_d, float* Ls)
+// (thread (r, g) holds T(r, g + 4i), i < 16).  Returns the first failing
+// column or -1 (uniform over the CTA).
+__device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_d)
 {
     const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
     float a[16];
@@ -174,36 +169,45 @@ __device__ int potf2_tile(float* T, long long ld, int nb, float* lcol, float* s_
     for (int i = 0; i < 16; ++i) {
         const int c = g + 4 * i;
         if (r < nb && c < nb && r >= c) T[(long long)c * ld + r] = a[i];
-        Ls[r * 65 + c] = a[i];  // zero outside the factor's lower triangle
     }
     return failed_at;
 }
 
-// D = L^{-1} for the nb x nb lower factor held zero-padded to 64 x 64 in Ls
-// (Ls[r * 65 + c]); the padding's diagonal counts as one.  Forward
-// substitution on the columns of D, four threads of one warp per column
-// (thread (t, q) keeps the rows i = q mod 4 of column t in Xs[i * 65 + t]);
-// per step k the owner of row k divides and the warp synchronises.  D is
-// written column-major with leading dimension 64 (D[c * 64 + r]).
-__device__ void tri_inv_tile(const float* Ls, int nb, float* Xs /*64 x 65*/, float* D)
+// D = L^{-1} for the nb x nb lower tile L (padded with the identity to 64):
+// thread t < 64 solves L x = e_t by forward substitution over a shared copy.
+// D is written column-major with leading dimension 64 (D[c * 64 + r]).
+__device__ void tri_inv_tile(const float* L, long long ld, int nb, float* Ls /*64 x 65*/,
+                             float* D)
 {
-    const int tid = threadIdx.x;
-    const int t = tid >> 2, q = tid & 3;  // column, row class
-    for (int i = q; i < kT; i += 4) Xs[i * 65 + t] = (i == t) ? 1.f : 0.f;
-    __syncwarp();
-    for (int k = 0; k < kT; ++k) {
-        const float dk = k < nb ? Ls[k * 65 + k] : 1.f;
-        if ((k & 3) == q) Xs[k * 65 + t] = Xs[k * 65 + t] / dk;
-        __syncwarp();
-        const float xk = Xs[k * 65 + t];
-        const int first = k + 1 + ((q - (k + 1)) & 3);  // first row > k of class q
-        for (int i = first; i < kT; i += 4) Xs[i * 65 + t] = fmaf(-Ls[i * 65 + k], xk, Xs[i * 65 + t]);
-        __syncwarp();
+    {
+        float v[kT * kT / kThreads];  // all loads in flight before the first store
+#pragma unroll
+        for (int u = 0; u < kT * kT / kThreads; ++u) {
+            const int q = threadIdx.x + u * kThreads, c = q >> 6, r = q & 63;
+            v[u] = (r < nb && c < nb && r >= c) ? __ldcg(L + (long long)c * ld + r) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < kT * kT / kThreads; ++u) {
+            const int q = threadIdx.x + u * kThreads, c = q >> 6, r = q & 63;
+            Ls[r * 65 + c] = v[u];
+        }
     }
     __syncthreads();
-    for (int e = tid; e < kT * kT; e += kThreads) {
-        const int c = e >> 6, r = e & 63;
-        D[e] = Xs[r * 65 + c];
+    const int t = threadIdx.x;
+    if (t < kT) {
+        float x[kT];
+#pragma unroll
+        for (int i = 0; i < kT; ++i) x[i] = (i == t) ? 1.f : 0.f;
+#pragma unroll
+        for (int k = 0; k < kT; ++k) {
+            if (k < nb) {
+                x[k] = x[k] / Ls[k * 65 + k];
+#pragma unroll
+                for (int i = k + 1; i < kT; ++i) x[i] = fmaf(-Ls[i * 65 + k], x[k], x[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kT; ++i) D[t * kT + i] = x[i];  // column t
     }
     __syncthreads();
 }
@@ -238,7 +242,7 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
 
     // Factor (and invert) diagonal tile k on this CTA; false on a bad pivot.
     auto factor_diag = [&](int k) -> bool {
-        const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d, As);
+        const int f = potf2_tile(tile(k, k), lda, ext(k), lcol, &s_d);
         if (f >= 0) {
             if (tid == 0) {
                 if (info) atomicCAS(info, 0, info_base + k * kT + f + 1);
@@ -247,7 +251,7 @@ potrf_block_kernel(int n, float* A, long long lda, int* info, int info_base, flo
             return false;
         }
         __syncthreads();
-        tri_inv_tile(As, ext(k), Bs, dinv + (long long)k * kT * kT);
+        tri_inv_tile(tile(k, k), lda, ext(k), As, dinv + (long long)k * kT * kT);
         return true;
     };
     // A(i,j) -= L(i,k) L(j,k)^T (lower part only on the diagonal)
