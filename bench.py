@@ -901,8 +901,8 @@ def run_ours(args, rank, world):
     mixed = None
     if not args.skip_mixed and world == 1:
         cases = [("spd", 1e2, "bf16", "ir"), ("spd", 1e2, "fp16", "ir"),
-                 ("gen", 1e2, "fp16", "gmres"), ("gen", 1e2, "bf16", "gmres"),
-                 ("gen", 1e2, "fp16x3", "ir"), ("gen", 1e4, "fp16", "gmres"),
+                 ("gen", 1e2, "fp16", "gmres"), ("gen", 1e2, "bf16", "auto"),
+                 ("gen", 1e2, "fp16x3", "ir"), ("gen", 1e4, "fp16", "auto"),
                  ("spd", 1e6, "fp16x3", "ir"), ("gen", 1e6, "fp16x3", "gmres")]
         mixed = mixed_ir_cases(torch, hd, handle, n, cases)
         best = {}
