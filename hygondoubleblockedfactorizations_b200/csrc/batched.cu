@@ -196,15 +196,32 @@ __device__ int chol_panel(Smem<T, PW>& s, int m, int kb)
     return 0;
 }
 
-// P (m x kb) <-> global A at the panel's top-left corner, column by column.
+// P (m x kb) <-> global A at the panel's top-left corner (element e is row
+// e % m of column e / m: coalesced), eight loads in flight per thread.
 template <int T, int PW, bool TO_SMEM>
 __device__ __forceinline__ void move_panel(Smem<T, PW>& s, float* A, long long lda, int m, int kb)
 {
-    for (int c = 0; c < kb; ++c)
-        for (int r = threadIdx.x; r < m; r += T) {
-            if (TO_SMEM) s.P[c * kLdp + r] = A[(long long)c * lda + r];
-            else A[(long long)c * lda + r] = s.P[c * kLdp + r];
+    const int total = m * kb;
+    int e = threadIdx.x;
+    for (; e + 7 * T < total; e += 8 * T) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = e + u * T, c = q / m, r = q - c * m;
+            v[u] = TO_SMEM ? A[(long long)c * lda + r] : s.P[c * kLdp + r];
         }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = e + u * T, c = q / m, r = q - c * m;
+            if (TO_SMEM) s.P[c * kLdp + r] = v[u];
+            else A[(long long)c * lda + r] = v[u];
+        }
+    }
+    for (; e < total; e += T) {
+        const int c = e / m, r = e - c * m;
+        if (TO_SMEM) s.P[c * kLdp + r] = A[(long long)c * lda + r];
+        else A[(long long)c * lda + r] = s.P[c * kLdp + r];
+    }
 }
 
 // --------------------------------------------------------- trailing update
@@ -306,37 +323,68 @@ __device__ int lu_factor(Smem<T, PW>& s, float* A, int n, long long lda, int* ip
         __syncthreads();
         const int nm = s_nm;
         // apply the moves to the columns left and right of the panel: one warp
-        // per column, every source read before any target is written
-        for (int c = warp; c < n - kb; c += T / 32) {
-            const int col = c < k ? c : c + kb;
-            float* Ac = A + (long long)col * lda + k;
-            float v0 = 0.f, v1 = 0.f;
-            if (lane < nm) v0 = Ac[s.mv[lane]];
-            if (lane + 32 < nm) v1 = Ac[s.mv[lane + 32]];
+        // per column, four columns per pass, every source of a column read
+        // before any of its targets is written
+        const int src0 = lane < nm ? s.mv[lane] : 0, src1 = lane + 32 < nm ? s.mv[lane + 32] : 0;
+        const int tgt0 = lane < nm ? s.mv[2 * PW + lane] : 0;
+        const int tgt1 = lane + 32 < nm ? s.mv[2 * PW + lane + 32] : 0;
+        for (int c = warp; c < n - kb; c += 4 * (T / 32)) {
+            float v0[4], v1[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int cu = c + u * (T / 32);
+                v0[u] = v1[u] = 0.f;
+                if (cu < n - kb) {
+                    const float* Ac = A + (long long)(cu < k ? cu : cu + kb) * lda + k;
+                    if (lane < nm) v0[u] = Ac[src0];
+                    if (lane + 32 < nm) v1[u] = Ac[src1];
+                }
+            }
             __syncwarp();
-            if (lane < nm) Ac[s.mv[2 * PW + lane]] = v0;
-            if (lane + 32 < nm) Ac[s.mv[2 * PW + lane + 32]] = v1;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int cu = c + u * (T / 32);
+                if (cu < n - kb) {
+                    float* Ac = A + (long long)(cu < k ? cu : cu + kb) * lda + k;
+                    if (lane < nm) Ac[tgt0] = v0[u];
+                    if (lane + 32 < nm) Ac[tgt1] = v1[u];
+                }
+            }
         }
         __syncthreads();
         const int m2 = m - kb;  // trailing rows / columns
+        // U12 = L11^{-1} A12 (unit lower) for every trailing column at once,
+        // one thread per column
+        for (int c = tid; c < m2; c += T) {
+            float* colp = A + (long long)(k + kb + c) * lda + k;
+            float xv[PW];
+#pragma unroll
+            for (int q = 0; q < PW; ++q) xv[q] = q < kb ? colp[q] : 0.f;
+#pragma unroll
+            for (int q = 0; q < PW; ++q)
+#pragma unroll
+                for (int r = q + 1; r < PW; ++r) xv[r] = fmaf(-s.P[q * kLdp + r], xv[q], xv[r]);
+#pragma unroll
+            for (int q = 0; q < PW; ++q)
+                if (q < kb) colp[q] = xv[q];
+        }
+        __syncthreads();
         for (int c0 = 0; c0 < m2; c0 += kChunk) {
             const int cw = min(kChunk, m2 - c0);
-            // U12 chunk = L11^{-1} A12 (unit lower), one thread per column
-            if (tid < cw) {
-                float* colp = A + (long long)(k + kb + c0 + tid) * lda + k;
-                float xv[PW];
+            // the chunk's U12 block into shared memory, all loads in flight
+            constexpr int kPer = (PW * kChunk + T - 1) / T;
+            float v[kPer];
 #pragma unroll
-                for (int q = 0; q < PW; ++q) xv[q] = q < kb ? colp[q] : 0.f;
+            for (int u = 0; u < kPer; ++u) {
+                const int e = threadIdx.x + u * T, c = e / PW, q = e - c * PW;
+                v[u] = (e < PW * kChunk && c < cw && q < kb)
+                           ? A[(long long)(k + kb + c0 + c) * lda + k + q]
+                           : 0.f;
+            }
 #pragma unroll
-                for (int q = 0; q < PW; ++q)
-#pragma unroll
-                    for (int r = q + 1; r < PW; ++r) xv[r] = fmaf(-s.P[q * kLdp + r], xv[q], xv[r]);
-#pragma unroll
-                for (int q = 0; q < PW; ++q)
-                    if (q < kb) {
-                        colp[q] = xv[q];
-                        s.Ub[q * kUbLd + tid] = xv[q];
-                    }
+            for (int u = 0; u < kPer; ++u) {
+                const int e = threadIdx.x + u * T, c = e / PW, q = e - c * PW;
+                if (e < PW * kChunk) s.Ub[q * kUbLd + c] = v[u];
             }
             __syncthreads();
             update_chunk<T, PW>(s, kb, m2, kb, s.Ub, kUbLd, cw,
@@ -416,8 +464,13 @@ __device__ void forward_lower(const float* A, int n, long long lda, float* x, bo
         }
         __syncthreads();
         for (int r = k + kb + tid; r < n; r += T) {
+            float a[PW];  // the row's block entries, all loads in flight together
+#pragma unroll
+            for (int q = 0; q < PW; ++q) a[q] = q < kb ? A[(long long)(k + q) * lda + r] : 0.f;
             float acc = x[r];
-            for (int q = 0; q < kb; ++q) acc = fmaf(-A[(long long)(k + q) * lda + r], x[k + q], acc);
+#pragma unroll
+            for (int q = 0; q < PW; ++q)
+                if (q < kb) acc = fmaf(-a[q], x[k + q], acc);
             x[r] = acc;
         }
         __syncthreads();
@@ -451,8 +504,13 @@ __device__ void backward_upper(const float* A, int n, long long lda, float* x)
         }
         __syncthreads();
         for (int r = tid; r < k; r += T) {
+            float a[PW];  // the row's block entries, all loads in flight together
+#pragma unroll
+            for (int q = 0; q < PW; ++q) a[q] = q < kb ? A[(long long)(k + q) * lda + r] : 0.f;
             float acc = x[r];
-            for (int q = 0; q < kb; ++q) acc = fmaf(-A[(long long)(k + q) * lda + r], x[k + q], acc);
+#pragma unroll
+            for (int q = 0; q < PW; ++q)
+                if (q < kb) acc = fmaf(-a[q], x[k + q], acc);
             x[r] = acc;
         }
         __syncthreads();
@@ -472,6 +530,7 @@ __device__ void backward_lower_t(const float* A, int n, long long lda, float* x,
         for (int j = warp; j < kb; j += T / 32) {
             const float* cj = A + (long long)(k + j) * lda;
             float sum = 0.f;
+#pragma unroll 4
             for (int r = k + kb + lane; r < n; r += 32) sum = fmaf(cj[r], x[r], sum);
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
