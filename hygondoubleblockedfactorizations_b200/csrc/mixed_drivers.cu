@@ -257,16 +257,26 @@ hdbf_status potrf_panel_fallback(hdbf_context* ctx, float* A, long long lda, con
 }
 
 // Right-looking mixed Cholesky (lower) with block b; shadows in `arena`.
+// BF16 (one product, no per-panel scale) pairs the panels: the first panel of
+// a pair updates only the second panel's block column (K = b), and the
+// trailing matrix takes both panels at once (K = 2b) from one shadow that
+// holds the pair's columns side by side -- half the passes over the FP32
+// trailing matrix, whose read-modify-write bounds the tensor-core update at
+// K = b.  The other modes update after every panel.
 hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long lda, int n, int b,
                              int* info, char* arena)
 {
     const PrecInfo pi = prec_info(prec);
     if (pi.fmt < 0) return HDBF_STATUS_INVALID_VALUE;
-    const long long lds = pad8(b);
+    const bool pair = pi.fmt == kFmtBF16 && !pi.split && b % 8 == 0 && b < n;
+    // pair: shadow and TRSM scratch of n x pad8(2b) each, inside the four
+    // n x pad8(b) arrays of the arena
+    const long long lds = pair ? pad8(2 * b) : pad8(b);
     const size_t one = (size_t)n * lds * 2;
-    void* hi = arena;
-    void* lo = pi.split ? arena + one : nullptr;
-    void* scratch_lo = arena + one;
+    char* hi = arena;
+    char* lo = pi.split ? arena + one : nullptr;
+    char* scratch_hi = pair ? arena + one : hi;
+    char* scratch_lo = pair ? nullptr : arena + one;
     // FP16 shadows carry a per-panel power-of-two scale (FP16's range is
     // narrow); BF16 has FP32's exponent range and needs none.
     unsigned* slots = reinterpret_cast<unsigned*>(arena + mixed_slots_offset(n, b));
@@ -291,6 +301,8 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         const int tr = n - k - psz;
         float* Akk = at(A, lda, k, k);
         const bool inv_tc = trsm_on_tc(pi) && tr > 0 && psz <= potrf_block_max_n();
+        const bool second = pair && ((k / b) & 1);  // second panel of a pair
+        const int k0 = second ? k - b : k;            // the pair's first column
         if (inv_tc) {
             int* flag = fail_flags + k / b;
             cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream);
@@ -302,30 +314,41 @@ hdbf_status potrf_mixed_body(hdbf_context* ctx, int prec, float* A, long long ld
         }
         if (tr <= 0) continue;
         float* A21 = at(A, lda, k + psz, k);
-        // L21 = A21 L11^{-T} as one tensor-core GEMM with W = L11^{-1} from
-        // the diagonal-block kernel; A21 is rounded into the shadow and
-        // overwritten with the product.
+        float* C22 = at(A, lda, k + psz, k + psz);
+        // this panel's rows k + psz .. n in the shadow: pair mode keeps the
+        // pair's panels side by side, rows counted from the pair's first column
+        char* sh = pair ? hi + ((size_t)(k + psz - k0) * lds + (k - k0)) * 2 : hi;
         if (!inv_tc) {
             HDBF_TRY(trsm_rlt(ctx, tr, psz, Akk, lda, A21, lda));
-            if (slot) HDBF_TRY(panel_absmax(ctx, A21, lda, tr, psz, slot));
-            HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, 1.f, slot));
-            HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
-                               at(A, lda, k + psz, k + psz), lda, 1.f, true, slot, slot));
-            continue;
+        } else {
+            // L21 = A21 L11^{-T} as one tensor-core GEMM with W = L11^{-1}
+            // from the diagonal-block kernel; A21 is rounded into the scratch
+            // and overwritten with the product (B operand W: A21 W^T).
+            HDBF_TRY(convert_transpose16(ctx, tp.fmt, psz, psz, wb.W, wb.ldw, wb.wh,
+                                         tp.split ? wb.wl : nullptr, wb.ldws, 1.f));
+            HDBF_TRY(convert_transpose16(ctx, tp.fmt, tr, psz, A21, lda, scratch_hi,
+                                         tp.split ? scratch_lo : nullptr, lds, 1.f));
+            HDBF_TRY(zero_block(ctx, A21, lda, tr, psz));
+            HDBF_TRY(tc_update(ctx, tp, tr, psz, psz, scratch_hi, scratch_lo, lds, wb.wh, wb.wl,
+                               wb.ldws, A21, lda, -1.f, false));
         }
-        // W = L11^{-1} came with the diagonal factorization; the GEMM's B
-        // operand (N x K, K-major) is W itself, so A21 W^T = A21 L11^{-T}.
-        HDBF_TRY(convert_transpose16(ctx, tp.fmt, psz, psz, wb.W, wb.ldw, wb.wh,
-                                     tp.split ? wb.wl : nullptr, wb.ldws, 1.f));
-        HDBF_TRY(convert_transpose16(ctx, tp.fmt, tr, psz, A21, lda, hi,
-                                     tp.split ? scratch_lo : nullptr, lds, 1.f));
-        HDBF_TRY(zero_block(ctx, A21, lda, tr, psz));
-        HDBF_TRY(tc_update(ctx, tp, tr, psz, psz, hi, scratch_lo, lds, wb.wh, wb.wl, wb.ldws, A21,
-                           lda, -1.f, false));
         if (slot) HDBF_TRY(panel_absmax(ctx, A21, lda, tr, psz, slot));
-        HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, hi, lo, lds, 1.f, slot));
-        HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds,
-                           at(A, lda, k + psz, k + psz), lda, 1.f, true, slot, slot));
+        HDBF_TRY(convert_transpose16(ctx, pi.fmt, tr, psz, A21, lda, sh, pi.split ? lo : nullptr,
+                                     lds, 1.f, slot));
+        if (!pair) {
+            HDBF_TRY(tc_update(ctx, pi, tr, tr, psz, hi, lo, lds, hi, lo, lds, C22, lda, 1.f, true,
+                               slot, slot));
+        } else if (!second) {
+            // the pair's second panel only (its block column, lower on top)
+            const int nb2 = std::min(b, tr);
+            HDBF_TRY(tc_update(ctx, pi, tr, nb2, psz, sh, nullptr, lds, sh, nullptr, lds, C22,
+                               lda, 1.f, true, nullptr, nullptr));
+        } else {
+            // the trailing matrix: both panels of the pair, K = b + psz
+            char* pr = hi + (size_t)(k + psz - k0) * lds * 2;
+            HDBF_TRY(tc_update(ctx, pi, tr, tr, b + psz, pr, nullptr, lds, pr, nullptr, lds, C22,
+                               lda, 1.f, true, nullptr, nullptr));
+        }
     }
     return last_cuda(ctx);
 }
