@@ -559,8 +559,14 @@ __device__ void backward_lower_t(const float* A, int n, long long lda, float* x,
 }
 
 // ------------------------------------------------------------------ kernel
+// Register budget for two CTAs per SM at 256 threads and three at 128 (the
+// 16-column panel's shared footprint allows three): one matrix per CTA spends
+// much of its time at barriers, so co-resident CTAs fill the gaps.
+template <int T>
+constexpr int min_ctas() { return T >= 512 ? 1 : (T >= 256 ? 2 : 3); }
+
 template <int T, int PW>
-__global__ void __launch_bounds__(T) batched_factor_solve_kernel(BatchArgs a)
+__global__ void __launch_bounds__(T, min_ctas<T>()) batched_factor_solve_kernel(BatchArgs a)
 {
     extern __shared__ __align__(16) float sm[];
     Smem<T, PW> s(sm);
