@@ -931,13 +931,16 @@ def run_ours(args, rank, world):
         hd.lib().hdbf_spotrf_mixed(handle.ptr, hd.PREC["bf16"], ctypes.c_void_p(wl.spd.data_ptr()),
                                    n, n, 1024, ctypes.c_void_p(wl.info.data_ptr()))
         tprof = handle.profile_end()
-        tc = tprof.get("tc_gemm_sub_kernel")
+        tc = tprof.get("tc_gemm_kernels")
+        tc_name = ("tc_gemm_sub_kernel" if os.environ.get("HDBF_TC_KERNEL", "0").strip() not in ("", "0")
+                   else "tc_gemm_persistent_kernel")
         if tc:
             nl, tms, fl, by = tc
             ach = fl / (tms / 1e3) / 1e12
             mixed["tensor_roofline"] = {
-                "bound": "tensor", "kernel": "tc_gemm_sub_kernel", "workload":
-                f"BF16 mixed POTRF n={n} panel 1024 (trailing SYRK updates)",
+                "bound": "tensor", "kernel": tc_name, "workload":
+                f"BF16 mixed POTRF n={n} panel 1024 (all tcgen05 updates: narrow in-pair "
+                "updates and K=2048 trailing SYRK updates)",
                 "achieved": round(ach, 1), "peak": tc_peak, "unit": "TFLOP/s",
                 "frac": round(ach / tc_peak, 4), "launches": nl,
                 "avg_launch_ms": round(tms / nl, 4),

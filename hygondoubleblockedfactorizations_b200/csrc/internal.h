@@ -19,7 +19,7 @@ enum KernelClass {
     kClsCompose = 5,  // compose_swaps_kernel
     kClsMoves = 6,    // apply_moves kernels
     kClsTrsmInv = 7,  // tri_inv64_kernel
-    kClsTcGemm = 8,   // tc_gemm_sub_kernel (tcgen05 mixed-precision updates)
+    kClsTcGemm = 8,   // tc_gemm_persistent_kernel / tc_gemm_sub_kernel (tcgen05 updates)
     kClsConvert = 9,  // FP32 -> 16-bit shadow conversions
     kClsIr = 10,      // FP64 residual / update / norm kernels
     kClsOther = 11,

@@ -631,7 +631,7 @@ const char* hdbf_profile_class_name(int cls)
                                              "rlt_apply_kernel", "llu_apply_kernel",
                                              "getf2_panel_kernel", "compose_swaps_kernel",
                                              "apply_moves", "tri_inv64_kernel",
-                                             "tc_gemm_sub_kernel", "convert16_kernels",
+                                             "tc_gemm_kernels", "convert16_kernels",
                                              "ir_fp64_kernels", "other",
                                              "trsv_wave_kernel", "sgemm_skinny_kernel",
                                              "batched_factor_solve_kernel",

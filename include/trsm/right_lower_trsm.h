@@ -27,8 +27,7 @@ void trsm_right_lower_transpose(hdbf_handle handle, int rows, int cols, const fl
  * process exits.  cols > HDBF_NOALLOC_TRSM_MAX_COLS returns
  * HDBF_STATUS_INVALID_VALUE and leaves B untouched.  The first call on a
  * device looks up that array's device address (cudaGetSymbolAddress) with the
- * device current, so make the first call on each device before any stream
- * capture.  All calls share the one array and leave their last contents in
+ * device current.  All calls share the one array and leave their last contents in
  * it; calls that overlap on the GPU (different streams, or different host
  * threads without ordering) race on it. */
 hdbf_status trsm_right_lower_transpose_noalloc(int rows, int cols, const float* A, int lda,
