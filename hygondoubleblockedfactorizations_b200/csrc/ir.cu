@@ -629,8 +629,8 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
 // one at least halves the backward error; from the first that does not,
 // GMRES steps on the same factors; when a GMRES step does not cut the
 // backward error tenfold, the factorization is redone at the next precision
-// (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3 -> FP32) and GMRES continues from
-// the current x.
+// (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3 -> FP32) and classical corrections
+// with the new factors continue from the current x, again until they stall.
 hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, int lda, int n,
                         int nrhs, const double* B, int ldb, double* X, int ldx, double tol,
                         int max_iter, int max_inner, double inner_tol, hdbf_ir_info* out,
@@ -750,6 +750,12 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             info.info = hinfo;
             info.fallback_panels = solver.fallbacks();
             if (st != HDBF_STATUS_SUCCESS || hinfo != 0) break;
+            // a classical correction costs two triangular solves against a
+            // GMRES step's several: use the new factors that way first
+            classical = true;
+            prev = berr;
+            st = timed(&info.refine_ms, [&] { return solver.correction(buf.R, n, true); });
+            continue;
         }
         prev = berr;
         // ---- inner GMRES on M^{-1} A d = M^{-1} r

@@ -99,8 +99,9 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, cons
  * GMRES-IR steps (30 inner steps, inner tolerance 1e-4) on the same factors;
  * when a GMRES step does not cut the backward error tenfold, the matrix is
  * refactored at the next precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3
- * -> FP32; also when the factorization itself fails) and GMRES continues
- * from the current solution.  Stops at tol or after max_iter outer steps;
+ * -> FP32; also when the factorization itself fails) and classical
+ * corrections with the new factors continue from the current solution, again
+ * until they stall.  Stops at tol or after max_iter outer steps;
  * out->final_precision and out->factorizations record the escalations.
  * nrhs <= 64. */
 hdbf_status hdbf_dposv_mixed_auto(hdbf_handle handle, hdbf_precision prec, const double* A,
