@@ -631,6 +631,9 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
 // backward error tenfold, the factorization is redone at the next precision
 // (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3 -> FP32) and classical corrections
 // with the new factors continue from the current x, again until they stall.
+// A general matrix factored with single-word BF16/FP16 updates skips the
+// GMRES stage: its stalled classical corrections lead straight to the split
+// (x3) factorization.
 hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, int lda, int n,
                         int nrhs, const double* B, int ldb, double* X, int ldx, double tol,
                         int max_iter, int max_inner, double inner_tol, hdbf_ir_info* out,
@@ -735,6 +738,7 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             break;
         }
         if (it >= max_iter) break;
+        bool refactor = false;
         if (classical) {
             if (berr < 0.5 * prev) {
                 prev = berr;
@@ -743,7 +747,15 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
                 continue;
             }
             classical = false;  // stalled: GMRES on the same factors from here
-        } else if (adaptive && !(berr < 0.1 * prev) && next_precision(cur) >= 0) {
+            // except on a single-word 16-bit LU, whose error grows with sqrt(n)
+            // and the pivot growth: restarted GMRES (30 steps) on such factors
+            // stalled at n = 32768 (BF16 at kappa 1e2, FP16 at kappa 1e4), so
+            // refactor with the split operands at once
+            refactor = !spd && (cur == HDBF_PREC_BF16 || cur == HDBF_PREC_FP16);
+        } else {
+            refactor = adaptive && !(berr < 0.1 * prev);
+        }
+        if (refactor && next_precision(cur) >= 0) {
             cur = next_precision(cur);
             st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
             info.factorizations++;

@@ -101,7 +101,10 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, cons
  * refactored at the next precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3
  * -> FP32; also when the factorization itself fails) and classical
  * corrections with the new factors continue from the current solution, again
- * until they stall.  Stops at tol or after max_iter outer steps;
+ * until they stall.  hdbf_dgesv_mixed_auto with BF16 or FP16 skips the GMRES
+ * stage on those single-word factors: when their classical corrections stall
+ * it refactors with the split operands (x3) at once.  Stops at tol or after
+ * max_iter outer steps;
  * out->final_precision and out->factorizations record the escalations.
  * nrhs <= 64. */
 hdbf_status hdbf_dposv_mixed_auto(hdbf_handle handle, hdbf_precision prec, const double* A,
