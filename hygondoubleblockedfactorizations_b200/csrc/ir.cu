@@ -627,10 +627,11 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
 // Givens least squares on the host per right-hand side), x += d.
 // Adaptive mode (`adaptive`): classical corrections d = M^{-1} r while each
 // one at least halves the backward error; from the first that does not,
-// GMRES steps on the same factors; when a GMRES step does not cut the
-// backward error tenfold, the factorization is redone at the next precision
-// (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3 -> FP32) and classical corrections
-// with the new factors continue from the current x, again until they stall.
+// GMRES steps on the same factors; when a GMRES step does not halve the
+// backward error, or its rate would need more time than two factorizations
+// to reach tol, the factorization is redone at the next precision (BF16 -> BF16x3 -> FP32,
+// FP16 -> FP16x3 -> FP32) and classical corrections with the new factors
+// continue from the current x, again until they stall.
 // A general matrix factored with single-word BF16/FP16 updates skips the
 // GMRES stage: its stalled classical corrections lead straight to the split
 // (x3) factorization.
@@ -714,11 +715,16 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             info.fallback_panels = solver.fallbacks();
         }
     }
+    // device time of the latest factorization and of the latest GMRES outer
+    // step (residual + inner iterations): the escalation test weighs them
+    double last_factor_ms = info.factorizations > 0 ? info.factor_ms / info.factorizations : 0.0;
+    double last_step_ms = 0.0;
     if (st == HDBF_STATUS_SUCCESS && hinfo == 0)
         st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });
     bool classical = adaptive;
     double prev = INFINITY;
     for (int it = 0; st == HDBF_STATUS_SUCCESS && hinfo == 0; ++it) {
+        const double step_start = info.refine_ms;
         st = timed(&info.refine_ms, [&] { return solver.residual(); });
         if (st != HDBF_STATUS_SUCCESS) break;
         st = solver.host_colmax(buf.R, n, rnorm.data());
@@ -752,12 +758,25 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             // stalled at n = 32768 (BF16 at kappa 1e2, FP16 at kappa 1e4), so
             // refactor with the split operands at once
             refactor = !spd && (cur == HDBF_PREC_BF16 || cur == HDBF_PREC_FP16);
-        } else {
-            refactor = adaptive && !(berr < 0.1 * prev);
+        } else if (adaptive) {
+            // after a GMRES step: refactor when it did not halve the backward
+            // error, or when the steps still needed at its rate would take
+            // longer than two factorizations at the current precision (the
+            // next precision's factorization costs 1.1x to 2.3x the current
+            // one on B200)
+            const double rate = berr / prev;
+            if (!(rate < 0.5)) {
+                refactor = true;
+            } else {
+                const double need = std::ceil(std::log(tol / berr) / std::log(rate));
+                refactor = need * last_step_ms > 2.0 * last_factor_ms;
+            }
         }
         if (refactor && next_precision(cur) >= 0) {
             cur = next_precision(cur);
+            const double f0 = info.factor_ms;
             st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
+            last_factor_ms = info.factor_ms - f0;
             info.factorizations++;
             info.info = hinfo;
             info.fallback_panels = solver.fallbacks();
@@ -841,6 +860,7 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             return solver.combine(buf.V, steps, buf.Yd);
         });
         info.inner_iterations += steps;
+        last_step_ms = info.refine_ms - step_start;
     }
     info.final_precision = cur;
     cudaEventDestroy(e0);

@@ -97,8 +97,9 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, cons
  * higher factorization precision.  Classical corrections d = M^{-1} r while
  * each at least halves the backward error; from the first that does not,
  * GMRES-IR steps (30 inner steps, inner tolerance 1e-4) on the same factors;
- * when a GMRES step does not cut the backward error tenfold, the matrix is
- * refactored at the next precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3
+ * when a GMRES step does not halve the backward error, or the steps still
+ * needed at its rate would take longer than two factorizations (device times
+ * measured during the call), the matrix is refactored at the next precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3
  * -> FP32; also when the factorization itself fails) and classical
  * corrections with the new factors continue from the current solution, again
  * until they stall.  hdbf_dgesv_mixed_auto with BF16 or FP16 skips the GMRES
