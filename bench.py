@@ -416,7 +416,9 @@ def mixed_ir_cases(torch, hd, handle, n, cases, nrhs=16, seed=2026):
                 "backward_error": float(info.backward_error),
                 "final_precision": int(info.final_precision),
                 "factorizations": int(info.factorizations),
-                "factor_ms": round(info.factor_ms, 2), "refine_ms": round(info.refine_ms, 2)}
+                "factor_ms": round(info.factor_ms, 2), "refine_ms": round(info.refine_ms, 2),
+                "history": [float(f"{info.history[i]:.3e}")
+                            for i in range(min(64, int(info.iterations) + 1))]}
 
     fp32_done = {}
     for kind, kappa, prec, method in cases:

@@ -577,6 +577,7 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
             st = timed(&info.refine_ms, [&] { return solver.correction(B, ldb, false); });
         double prev = INFINITY;
         int stalls = 0;
+        bool refactored = false;
         for (int it = 0; st == HDBF_STATUS_SUCCESS && hinfo == 0; ++it) {
             st = timed(&info.refine_ms, [&] { return solver.residual(); });
             if (st != HDBF_STATUS_SUCCESS) break;
@@ -607,11 +608,17 @@ hdbf_status xsv_mixed(hdbf_context* ctx, bool spd, int prec, int escalate, const
                     info.fallback_panels = solver.fallbacks();
                     if (hinfo2 != 0) break;
                     stalls = 0;
+                    // the first correction with the new factors is not
+                    // judged: forward error that the old factors left along
+                    // the smallest singular directions shows up in the
+                    // backward error only after it has been spread out
+                    refactored = true;
                 } else if (++stalls >= 2) {
                     break;
                 }
             }
-            prev = std::min(prev, berr);
+            prev = refactored ? INFINITY : std::min(prev, berr);
+            refactored = false;
             st = timed(&info.refine_ms, [&] { return solver.correction(solver.buffers().R, n, true); });
         }
     }
@@ -782,9 +789,12 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
             info.fallback_panels = solver.fallbacks();
             if (st != HDBF_STATUS_SUCCESS || hinfo != 0) break;
             // a classical correction costs two triangular solves against a
-            // GMRES step's several: use the new factors that way first
+            // GMRES step's several: use the new factors that way first.  The
+            // first correction is not judged (prev = inf): forward error that
+            // the old factors left along the smallest singular directions
+            // shows up in the backward error only after it has been spread out
             classical = true;
-            prev = berr;
+            prev = INFINITY;
             st = timed(&info.refine_ms, [&] { return solver.correction(buf.R, n, true); });
             continue;
         }

@@ -69,7 +69,8 @@ typedef struct hdbf_ir_info {
  * refinement x += A^{-1}(b - A x) runs with FP64 residuals.  With `escalate`,
  * a step that does not halve the backward error (or a failed factorization)
  * refactors at the next precision (BF16 -> BF16X3 -> FP32, FP16 -> FP16X3 ->
- * FP32).  nrhs <= 64.  X may alias nothing else. */
+ * FP32); the first step with the new factors is taken without that test.
+ * nrhs <= 64.  X may alias nothing else. */
 hdbf_status hdbf_dposv_mixed(hdbf_handle handle, hdbf_precision prec, int escalate,
                              const double* A, int lda, int n, int nrhs, const double* B, int ldb,
                              double* X, int ldx, double tol, int max_iter, hdbf_ir_info* out);
@@ -94,20 +95,23 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, cons
                                    double inner_tol, hdbf_ir_info* out);
 
 /* Adaptive refinement: one call that picks the refinement and, if needed, a
- * higher factorization precision.  Classical corrections d = M^{-1} r while
- * each at least halves the backward error; from the first that does not,
- * GMRES-IR steps (30 inner steps, inner tolerance 1e-4) on the same factors;
- * when a GMRES step does not halve the backward error, or the steps still
- * needed at its rate would take longer than two factorizations (device times
- * measured during the call), the matrix is refactored at the next precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3
- * -> FP32; also when the factorization itself fails) and classical
- * corrections with the new factors continue from the current solution, again
- * until they stall.  hdbf_dgesv_mixed_auto with BF16 or FP16 skips the GMRES
- * stage on those single-word factors: when their classical corrections stall
- * it refactors with the split operands (x3) at once.  Stops at tol or after
- * max_iter outer steps;
- * out->final_precision and out->factorizations record the escalations.
- * nrhs <= 64. */
+ * higher factorization precision.
+ *  - Classical corrections d = M^{-1} r while each at least halves the
+ *    backward error.
+ *  - From the first that does not, GMRES-IR steps (30 inner steps, inner
+ *    tolerance 1e-4) on the same factors.
+ *  - When a GMRES step does not halve the backward error, or the steps still
+ *    needed at its rate would take longer than two factorizations (device
+ *    times measured during the call), the matrix is refactored at the next
+ *    precision (BF16 -> BF16x3 -> FP32, FP16 -> FP16x3 -> FP32; also when the
+ *    factorization itself fails).  Classical corrections with the new factors
+ *    continue from the current solution (the first one is not judged), again
+ *    until they stall.
+ *  - hdbf_dgesv_mixed_auto with BF16 or FP16 skips the GMRES stage on those
+ *    single-word factors: when their classical corrections stall it refactors
+ *    with the split operands (x3) at once.
+ * Stops at tol or after max_iter outer steps; out->final_precision and
+ * out->factorizations record the escalations.  nrhs <= 64. */
 hdbf_status hdbf_dposv_mixed_auto(hdbf_handle handle, hdbf_precision prec, const double* A,
                                   int lda, int n, int nrhs, const double* B, int ldb, double* X,
                                   int ldx, double tol, int max_iter, hdbf_ir_info* out);
