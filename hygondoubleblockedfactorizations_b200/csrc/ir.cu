@@ -311,6 +311,16 @@ int next_precision(int prec)
     }
 }
 
+// The adaptive driver's escalation: as next_precision, except that an LU
+// factored with BF16 updates goes to the FP16 split (22 significant bits
+// against BF16x3's 16, at the same cost; |L| <= 1 under partial pivoting and
+// U's shadow carries a per-panel power-of-two scale, so FP16 covers the range)
+int adaptive_next(bool spd, int prec)
+{
+    if (!spd && prec == HDBF_PREC_BF16) return HDBF_PREC_FP16X3;
+    return next_precision(prec);
+}
+
 // Block sizes of the refinement's factorization: the fastest candidates of
 // the exhaustive B200 sweep over n = 1024..32768 (the selector's training
 // records).  FP32 POTRF: (2048, 256) below n = 16384, else (4096, 512).
@@ -713,9 +723,9 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
     }
     int cur = prec;
     if (adaptive) {
-        while (st == HDBF_STATUS_SUCCESS && hinfo != 0 && next_precision(cur) >= 0) {
+        while (st == HDBF_STATUS_SUCCESS && hinfo != 0 && adaptive_next(spd, cur) >= 0) {
             // the panel fallback could not save it: refactor at the next precision
-            cur = next_precision(cur);
+            cur = adaptive_next(spd, cur);
             st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
             info.factorizations++;
             info.info = hinfo;
@@ -779,8 +789,8 @@ hdbf_status gmres_mixed(hdbf_context* ctx, bool spd, int prec, const double* A, 
                 refactor = need * last_step_ms > 2.0 * last_factor_ms;
             }
         }
-        if (refactor && next_precision(cur) >= 0) {
-            cur = next_precision(cur);
+        if (refactor && adaptive_next(spd, cur) >= 0) {
+            cur = adaptive_next(spd, cur);
             const double f0 = info.factor_ms;
             st = timed(&info.factor_ms, [&] { return solver.factor(cur, &hinfo); });
             last_factor_ms = info.factor_ms - f0;

@@ -109,7 +109,8 @@ hdbf_status hdbf_dgesv_mixed_gmres(hdbf_handle handle, hdbf_precision prec, cons
  *    until they stall.
  *  - hdbf_dgesv_mixed_auto with BF16 or FP16 skips the GMRES stage on those
  *    single-word factors: when their classical corrections stall it refactors
- *    with the split operands (x3) at once.
+ *    with the FP16 split (FP16x3) at once, from BF16 too (22 significant bits
+ *    against BF16x3's 16, at the same cost).
  * Stops at tol or after max_iter outer steps; out->final_precision and
  * out->factorizations record the escalations.  nrhs <= 64. */
 hdbf_status hdbf_dposv_mixed_auto(hdbf_handle handle, hdbf_precision prec, const double* A,

@@ -272,6 +272,7 @@ def test_dgesv_mixed_auto_escalates(hd, handle, torch_cuda, prec):
     assert info.converged == 1, (info.backward_error, list(info.history[:info.iterations + 1]),
                                  info.final_precision, info.factorizations)
     assert oracle.backward_error(A, X, B) <= 1e-13
-    chain = [prec, prec + "x3", "fp32"]  # the escalation order
+    # the LU escalation order: BF16 goes to the FP16 split (more significant bits)
+    chain = [prec, "fp16x3", "fp32"]
     assert info.final_precision == hd_mod.PREC[chain[info.factorizations - 1]], \
         (info.final_precision, info.factorizations)
